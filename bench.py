@@ -1,0 +1,369 @@
+"""Benchmark of the displacement hot path: atoms/s with all loops and images.
+
+Default workload: fcc_random (FCC a0 3.615 A, 150^3 cells = 13.5 M atoms, 64
+glide loops = 1696 segments, images +-2 = 125, nu 0.34), FP64 line method, one
+GPU.  A step is one full displacement sum over all atoms.
+
+  value   device-resident: positions and displacements already in HBM, one
+          plan execute per step (CUDA events on the launching stream, max over
+          ranks).  Inputs (324 MB of positions) are larger than L2.
+  e2e     the public host call (kroupa_gpu, the kroupaGPU drop-in) on pinned
+          host arrays: table build, allocation, H2D of positions and
+          displacements, kernel, D2H of the displacements, per step.
+  roofline  W = 128 flop per segment-image evaluation (66 per loopon-image)
+          against the FP64 peak measured here with a DGEMM (the driver's peak
+          file has no FP64 figure); traffic from the committed ncu summary.
+  cpu_baseline  the oracle (CPU restatement, the reference's flags) on a
+          seeded atom sample, all host threads, rank 0 only.
+
+--impl reference times the reference's CPU implementation on the same
+workload: its own kroupaCPU compiled from its sources (oracle/_ref) where the
+workload has the reference's fixed images +-1, else the oracle restatement of
+it (images and nu are compile-time constants in the reference).
+
+Multi-GPU (torchrun): every rank runs the same workload on its own GPU
+(replicas, weak scaling, no collective on the data path); value = all ranks'
+atoms / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "atoms/s with all loops+images; learned/FP32 vs plain FP64 at max |Δu|≤1e-3 Å"
+W_LINE = 128.0     # flop per segment-image evaluation
+W_LOOPON = 66.0    # flop per loopon-image evaluation
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="fcc_random")
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
+    p.add_argument("--e2e-steps", type=int, default=None)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--image-split", type=int, default=0)
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), \
+        int(os.environ.get("LOCAL_RANK", 0))
+
+
+def build_workload(name):
+    from disco_b200 import workloads as W
+    return W.FULL[name]()
+
+
+def flop_per_eval(w):
+    return W_LINE if w.method == "line" else W_LOOPON
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (every 200 ms)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch):
+    """Dense FP64 throughput of this GPU, measured with a DGEMM (best of 5)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def traffic_from_profiles(kernel_key):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_key}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("traffic_per_launch_bytes:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_baseline(w, seconds, use_reference):
+    """Atoms/s of a CPU implementation on a seeded atom sample (all threads)."""
+    import oracle as O
+    rng = np.random.default_rng(1234)
+    threads = os.cpu_count() or 1
+    ref_ok = use_reference and w.images == 1 and O.have_ref()
+
+    def run(idx):
+        x, y, z = w.x[idx], w.y[idx], w.z[idx]
+        t0 = time.perf_counter()
+        if ref_ok:
+            u = O.ref_displace(x, y, z, w.loops, w.box)
+        else:
+            u = O.displace(x, y, z, w.loops, w.box, images=w.images, nu=w.nu, threads=threads)
+        return time.perf_counter() - t0, u
+
+    k = max(threads, 8)
+    idx = np.sort(rng.choice(w.n, size=min(k, w.n), replace=False))
+    dt, _ = run(idx)
+    rate = len(idx) / dt
+    k = int(min(w.n, max(len(idx), rate * seconds)))
+    idx = np.sort(rng.choice(w.n, size=k, replace=False))
+    dt, u = run(idx)
+    kind = "reference" if ref_ok else "port"
+    what = ("the reference's kroupaCPU compiled from its sources (oracle/_ref), nu fixed at 0.35 "
+            "in the reference, same operation count") if ref_ok else \
+        ("oracle restatement of kroupaCPU (Code/backend_cpu.cpp:28-99) with the workload's nu and "
+         "image range, built with the reference's flags")
+    return {"value": k / dt, "unit": "atoms/s", "cores": threads, "kind": kind,
+            "sample": f"{k} seeded random atoms of {w.n}, all {len(w.loops)} loops x "
+                      f"{(2 * w.images + 1) ** 3} images, {dt:.1f} s; {what}",
+            "seconds": dt}, idx, u
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    w = build_workload(args.config)
+    import oracle as O
+    threads = os.cpu_count() or 1
+    ref_ok = w.images == 1 and O.have_ref()
+    rng = np.random.default_rng(99)
+    # bounded sample per step so that warmup + steps stay within a few minutes
+    probe = np.sort(rng.choice(w.n, size=max(threads, 8), replace=False))
+    t0 = time.perf_counter()
+    if ref_ok:
+        O.ref_displace(w.x[probe], w.y[probe], w.z[probe], w.loops, w.box)
+    else:
+        O.displace(w.x[probe], w.y[probe], w.z[probe], w.loops, w.box, images=w.images, nu=w.nu,
+                   threads=threads)
+    rate = len(probe) / (time.perf_counter() - t0)
+    per_step = max(8.0, min(25.0, 150.0 / max(1, args.steps + args.warmup)))
+    k = int(min(w.n, max(len(probe), rate * per_step)))
+    times = []
+    for s in range(args.warmup + args.steps):
+        idx = np.sort(rng.choice(w.n, size=k, replace=False))
+        t0 = time.perf_counter()
+        if ref_ok:
+            O.ref_displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box)
+        else:
+            O.displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box, images=w.images, nu=w.nu,
+                       threads=threads)
+        if s >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    T = sum(times)
+    value = k * args.steps / T
+    kind = "reference" if ref_ok else "port"
+    sample = f"{k} seeded random atoms of {w.n} per step, all loops and images"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "atoms/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * T / args.steps * (w.n / k), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.config, "atoms": w.n, "loops": len(w.loops),
+                   "images": (2 * w.images + 1) ** 3, "nu": w.nu, "method": w.method},
+        "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": threads, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from disco_b200 import backend as B
+    from disco_b200 import _capi as C
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    w = build_workload(args.config)
+    prec = C.DISCO_FP32C if args.precision == "fp32c" else C.DISCO_FP64
+    n = w.n
+    plan = B.Plan(w.loops, w.box, precision=prec, images=w.images, nu=w.nu,
+                  image_split=args.image_split, max_atoms=n)
+    st = plan.stats()
+    evals_atom = st["evals_per_atom"]
+    stream = torch.cuda.current_stream()
+    pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
+    u = torch.zeros_like(pos)
+    launches_per_step = int(st["n_line_loops"] > 0) + int(st["n_loopon_loops"] > 0)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        plan.execute(pos, u)
+    plan.sync(stream.cuda_stream)
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.execute(pos, u)
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    plan.sync(stream.cuda_stream)
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    per_launch = elapsed / args.steps
+    value = n * world * args.steps / elapsed
+
+    # parity on a seeded sample (fresh sum) while the CPU baseline runs on it
+    u1 = torch.zeros_like(pos)
+    plan.execute(pos, u1)
+    plan.sync(stream.cuda_stream)
+    u1 = u1.cpu().numpy()
+
+    # e2e: the public host call on pinned host memory
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
+    hp = torch.empty((6, n), dtype=torch.float64, pin_memory=True)
+    hv = hp.numpy()
+    hv[0], hv[1], hv[2] = w.x, w.y, w.z
+    atoms = B.AtomArrays(hv[0], hv[1], hv[2], hv[3], hv[4], hv[5])
+    hv[3:] = 0.0
+    B.kroupa_gpu(atoms, w.loops, *w.box, B.GpuOptions(fp32=prec == C.DISCO_FP32C), images=w.images,
+                 nu=w.nu, image_split=args.image_split)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        hv[3:] = 0.0
+        B.kroupa_gpu(atoms, w.loops, *w.box, B.GpuOptions(fp32=prec == C.DISCO_FP32C),
+                     images=w.images, nu=w.nu, image_split=args.image_split)
+    barrier()
+    e2e_t = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_t], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e = {"value": n * world * e2e_steps / e2e_t, "unit": "atoms/s",
+           "h2d_bytes_per_step": 6 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n, "steps": e2e_steps}
+
+    if rank == 0:
+        peak = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else None
+        flops = evals_atom * n * flop_per_eval(w)
+        achieved = flops / per_launch / 1e12
+        key = f"{'line' if w.method == 'line' else 'loopon'}_{args.precision}_{args.config}"
+        traffic = traffic_from_profiles(key)
+        roof = {"bound": "fp64" if prec == C.DISCO_FP64 else "fp32", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s", "frac": (achieved / peak) if peak else None,
+                "traffic": traffic,
+                "peak_source": "measured here: torch DGEMM 8192^3 best of 5 (MEASURED_PEAKS.json has no "
+                               "FP64 figure)" if peak else None,
+                "flop_per_eval": flop_per_eval(w), "evals_per_launch": evals_atom * n}
+        cpu = None
+        parity = None
+        if not args.no_cpu:
+            cpu, idx, ucpu = cpu_baseline(w, args.cpu_seconds, use_reference=False)
+            du = np.abs(u1[:, idx] - np.stack(ucpu)).max()
+            parity = {"max_abs_du": float(du), "atoms": int(len(idx)), "against": "oracle"}
+            cpu.pop("seconds", None)
+        line = {
+            "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_launch,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == C.DISCO_FP64 else "f32c", "data": "synthetic",
+            "config": {"workload": args.config, "atoms": n, "loops": len(w.loops),
+                       "segments": st["n_segments"], "loopons": st["n_loopons"],
+                       "images": st["n_images"], "nu": w.nu, "method": w.method,
+                       "precision": args.precision, "l2": "inputs larger than L2 (positions "
+                       f"{24 * n / 1e6:.0f} MB)", "parallelism": f"replicas x{world}"},
+            "evals_per_s": evals_atom * n * world * args.steps / elapsed,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": launches_per_step * args.steps, "parity": parity,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

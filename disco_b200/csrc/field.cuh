@@ -1,0 +1,132 @@
+// Loop tables of the displacement sum and the launcher interface.
+//
+// A plan turns the caller's loops (disco_loop) into a device table cut into
+// "pieces" — a run of at most a few hundred segments (line method) or loopons
+// (loopon method) of one loop, with everything that does not depend on the
+// atom precomputed — packed into "chunks" that are staged whole into shared
+// memory.  Pieces are independent: the field of a loop is the sum of the
+// fields of its pieces (the solid angle of a convex fan splits into the solid
+// angles of its sub-fans, each below 2 pi in magnitude).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/disco_b200.h"
+
+namespace disco {
+
+constexpr int kLineKind = 0;
+constexpr int kLooponKind = 1;
+
+// ---- FP64 line method (Code/barnett.hpp:44-107) --------------------------------
+struct alignas(16) LinePiece {
+    double ax, ay, az;   // vertex before the piece's first segment
+    double cx, cy, cz;   // fan apex (loop centre)
+    double bx, by, bz;   // Burgers vector (phys.b * m)
+    int32_t nseg;        // segments of this piece
+    int32_t rec;         // first segment record, index into the chunk's records
+};
+struct alignas(16) LineSeg {
+    double vx, vy, vz;   // end vertex B of segment A -> B
+    double len;          // |B - A|
+    double tx, ty, tz;   // unit tangent (B - A) / |B - A| (0 for a null segment)
+    double wx, wy, wz;   // w = b x t
+};
+static_assert(sizeof(LinePiece) == 80 && sizeof(LineSeg) == 80, "line table layout");
+
+// ---- FP64 loopon method (Code/kroupa.hpp:52-73) ---------------------------------
+struct alignas(16) LooponPiece {
+    double cx, cy, cz;    // reference point of the loop (loopon centroid)
+    double fbx, fby, fbz; // -k1 dS b (Kroupa prefactor times the Burgers components)
+    double mx, my, mz;    // unit glide direction m
+    double nx, ny, nz;    // unit normal n
+    double b_n;           // m . n
+    int32_t n;            // loopons of this piece
+    int32_t rec;          // first loopon record in the chunk
+};
+struct alignas(16) LooponRec {
+    double x, y, z;       // loopon - reference point
+    double ml, nl;        // m . (loopon - c), n . (loopon - c)
+    double pad;
+};
+static_assert(sizeof(LooponPiece) == 112 && sizeof(LooponRec) == 48, "loopon table layout");
+
+// ---- FP32 compensated forms -------------------------------------------------------
+struct alignas(16) LinePieceF {
+    double cx, cy, cz;    // loop centre (FP64): atoms enter relative to it
+    float ax, ay, az;     // start vertex relative to the centre
+    float bx, by, bz;     // Burgers vector
+    int32_t nseg, rec;
+    int32_t pad0, pad1, pad2;   // 24 + 24 + 20 -> 80 B
+};
+struct alignas(16) LineSegF {
+    float vx, vy, vz, len;   // end vertex relative to the centre, length
+    float tx, ty, tz;        // unit tangent
+    float wx, wy, wz;        // b x t
+    float pad0, pad1;        // 48 B
+};
+static_assert(sizeof(LinePieceF) == 80 && sizeof(LineSegF) == 48, "fp32 line table layout");
+
+struct alignas(16) LooponPieceF {
+    double cx, cy, cz;      // reference point (FP64)
+    float fbx, fby, fbz;    // -k1 dS b
+    float mx, my, mz, nx, ny, nz;
+    float b_n;
+    int32_t n, rec;         // 24 + 48 + 8 = 80 B
+    int32_t pad0, pad1;
+};
+struct alignas(16) LooponRecF {
+    float x, y, z, ml;      // loopon - c, m . (loopon - c)
+    float nl, pad0, pad1, pad2;   // 32 B
+};
+static_assert(sizeof(LooponPieceF) == 80 && sizeof(LooponRecF) == 32, "fp32 loopon table layout");
+
+struct Chunk {
+    uint64_t offset;      // byte offset of the chunk in the table
+    uint32_t bytes;       // pieces then records, a multiple of 16
+    int32_t npieces;
+};
+
+// Everything one launch needs; passed by value.
+struct FieldArgs {
+    const double *x, *y, *z;
+    double *ux, *uy, *uz;
+    int64_t n;
+    const unsigned char* table;
+    const Chunk* chunks;
+    int32_t nchunks;
+    uint32_t stage_bytes;     // shared-memory bytes of one stage buffer
+    int32_t resident;         // one chunk, loaded once per CTA
+    int32_t images, nimg;     // image range and (2 images + 1)^3
+    double Lx, Ly, Lz;
+    double cJ, cK;            // line: c3 - 1/(4 pi), c3 = 1 / (8 pi (1 - nu))
+    double c2;                // loopon: 1 - 2 nu
+    int* status;
+};
+
+// Host-side table: bytes + chunk list, built once per plan.
+struct HostTable {
+    int kind = kLineKind;
+    bool fp32 = false;
+    std::vector<unsigned char> bytes;
+    std::vector<Chunk> chunks;
+    uint32_t stage_bytes = 0;
+    bool resident = false;
+    std::vector<double> loop_evals;   // evaluations per atom per image, per input loop
+    int64_t n_segments = 0, n_loopons = 0;
+};
+
+// Builds the table of the loops of one kind (kLineKind: loops with line != 0,
+// kLooponKind: the others); returns DISCO_OK or an error code.
+int build_table(const disco_loop* loops, int nloops, int kind, int precision, double nu,
+                HostTable& out, std::string& err);
+
+// Picks the image split factor and grid and launches the kernel on `stream`.
+int launch_field(const FieldArgs& args, int kind, bool fp32, int sm_count, int threads_hint,
+                 int split_hint, cudaStream_t stream, std::string& err);
+
+} // namespace disco

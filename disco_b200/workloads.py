@@ -1,0 +1,156 @@
+"""Seeded synthetic workloads of the displacement hot path.
+
+The reference's benchmarks are input files, not datasets; these builders make
+the same kind of input (lattice sites in generateLattice order, loop centres
+snapped to mid-planes, polylines and loopon grids from the loop class) with
+the shapes, sizes and distributions of each workload, from a numpy PCG64
+generator with a fixed seed.  Both the GPU path and the CPU oracle consume the
+arrays built here, so parity never depends on regenerating an input.
+
+  quadrupole        BCC a0 2.855, 40^3 cells (128 000 atoms), 4 circular glide
+                    loops R 30 A on {110}, b = a0/2<111> with alternating
+                    signs, centres at the quarter points, 64 chords each
+                    (Segment_tolerance 0.0365), nu 0.29, images +-1, line method
+  fcc_random        FCC a0 3.615, 150^3 cells (13.5 M atoms), 64 glide loops on
+                    random {111} with b = a0/2<110> in the plane: 32 circles R
+                    U(10, 40) of 48 chords, 16 hexagons circumradius U(15, 35),
+                    16 rectangles with sides U(20, 60); nu 0.34, images +-2
+  bcc_prismatic     BCC a0 3.165, 60^3 cells (432 000 atoms), 16 prismatic
+                    circles R U(20, 50) on {111} with b = a0/2<111> along n
+                    (8 interstitial, 8 vacancy), loopons on a 1 A grid, nu 0.28,
+                    images +-1, plus the slab loops of the matter step
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import geometry as G
+
+# {111} normals and the <110> directions in each of those planes
+_N111 = [(1, 1, 1), (-1, 1, 1), (1, -1, 1), (1, 1, -1)]
+_D110 = [(1, -1, 0), (1, 0, -1), (0, 1, -1), (1, 1, 0), (1, 0, 1), (0, 1, 1)]
+
+
+def _in_plane_110(n):
+    out = []
+    for d in _D110:
+        if d[0] * n[0] + d[1] * n[1] + d[2] * n[2] == 0:
+            out += [d, tuple(-t for t in d)]
+    return out
+
+
+@dataclass
+class Workload:
+    name: str
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    loops: list
+    box: tuple
+    images: int
+    nu: float
+    method: str                      # "line" or "loopons"
+    lattice: int = G.BCC
+    a0: float = 0.0
+    cells: tuple = (0, 0, 0)
+    slab_loops: list = field(default_factory=list)
+    geom: list = field(default_factory=list)
+
+    @property
+    def n(self):
+        return int(self.x.shape[0])
+
+    def evals_per_atom(self):
+        """(segments or loopons) x images, summed over the loops."""
+        k = sum(len(lp.vx) if lp.line else len(lp.x) for lp in self.loops)
+        return k * (2 * self.images + 1) ** 3
+
+    def subset(self, idx):
+        """The same loops and box over a subset of the atoms (sampling)."""
+        w = Workload(**{**self.__dict__})
+        w.x, w.y, w.z = self.x[idx].copy(), self.y[idx].copy(), self.z[idx].copy()
+        w.name = self.name + f"[{len(idx)} atoms]"
+        return w
+
+
+def quadrupole(cells=40, a0=2.855, radius=30.0, eps=0.0365, nu=0.29, images=1, da=1.0):
+    """Four circular shear loops forming a quadrupole (the pattern of the
+    reference's Examples/quadrupole_circle.yaml), line method."""
+    L = cells * a0
+    q = L / 4.0
+    specs = [((-q, -q, 0.0), (1, -1, -1), (1, 1, 0)),
+             ((-q, q, 0.0), (-1, -1, 1), (-1, 1, 0)),
+             ((q, -q, 0.0), (-1, -1, -1), (-1, 1, 0)),
+             ((q, q, 0.0), (1, -1, 1), (1, 1, 0))]
+    x, y, z = G.lattice(G.BCC, cells, cells, cells, a0)
+    loops, geom = [], []
+    for c, m, n in specs:
+        cs, _ = G.snap(c, n, a0, cells, cells, cells, G.BCC)
+        lp = G.Loop.circle(da, radius, cs, m, n, a0)
+        geom.append(lp)
+        loops.append(lp.line_data(eps))
+    return Workload("quadrupole", x, y, z, loops, (L, L, L), images, nu, "line", G.BCC, a0,
+                    (cells, cells, cells), geom=geom)
+
+
+def fcc_random(cells=150, a0=3.615, nu=0.34, images=2, seed=2, n_circles=32, n_hex=16, n_rect=16,
+               chords=48, da=1.0):
+    """64 random shear loops in an FCC box, line method."""
+    rng = np.random.default_rng(seed)
+    L = cells * a0
+    x, y, z = G.lattice(G.FCC, cells, cells, cells, a0)
+    loops, geom = [], []
+    kinds = ["circle"] * n_circles + ["hexagon"] * n_hex + ["rectangle"] * n_rect
+    for kind in kinds:
+        n = _N111[rng.integers(len(_N111))]
+        ms = _in_plane_110(n)
+        m = ms[rng.integers(len(ms))]
+        c = rng.uniform(-L / 2, L / 2, size=3)
+        cs, _ = G.snap(c, n, a0, cells, cells, cells, G.FCC)
+        if kind == "circle":
+            R = rng.uniform(10.0, 40.0)
+            lp = G.Loop.circle(da, R, cs, m, n, a0)
+            P = lp.polyline(G.circle_eps_for_chords(R, chords))
+        elif kind == "hexagon":
+            R = rng.uniform(15.0, 35.0)
+            lp = G.Loop.polygon(da, G.regular_polygon(6, R, m, n), 0.0, cs, m, n, a0)
+            P = lp.polyline(0.01)
+        else:
+            s1, s2 = rng.uniform(20.0, 60.0, size=2)
+            lp = G.Loop.rectangle(da, s1 / 2, s2 / 2, 0.0, cs, m, n, a0)
+            P = lp.polyline(0.01)
+        geom.append(lp)
+        loops.append(lp.line_data(vertices=P))
+    return Workload("fcc_random", x, y, z, loops, (L, L, L), images, nu, "line", G.FCC, a0,
+                    (cells, cells, cells), geom=geom)
+
+
+def bcc_prismatic(cells=60, a0=3.165, nu=0.28, images=1, seed=3, n_inter=8, n_vac=8, da=1.0,
+                  rmin=20.0, rmax=50.0):
+    """16 prismatic circular loops (loopon method) with their slab loops."""
+    rng = np.random.default_rng(seed)
+    L = cells * a0
+    x, y, z = G.lattice(G.BCC, cells, cells, cells, a0)
+    kinds = np.array(["inter"] * n_inter + ["vac"] * n_vac)
+    rng.shuffle(kinds)
+    loops, geom, slabs = [], [], []
+    for kind in kinds:
+        n = _N111[rng.integers(len(_N111))]
+        m = n if kind == "vac" else tuple(-t for t in n)      # m.n > 0: vacancy
+        R = rng.uniform(rmin, rmax)
+        c = rng.uniform(-L / 2, L / 2, size=3)
+        cs, d = G.snap(c, n, a0, cells, cells, cells, G.BCC)
+        lp = G.Loop.circle(da, R, cs, m, n, a0)
+        geom.append(lp)
+        loops.append(lp.loopon_data())
+        slabs.append(lp.slab_loop(d, apply=True, frank=False, a0=a0))
+    return Workload("bcc_prismatic", x, y, z, loops, (L, L, L), images, nu, "loopons", G.BCC, a0,
+                    (cells, cells, cells), slab_loops=slabs, geom=geom)
+
+
+# Full-size workloads by name (bench and tests select them by these names).
+FULL = {
+    "quadrupole": quadrupole,
+    "fcc_random": fcc_random,
+    "bcc_prismatic": bcc_prismatic,
+}

@@ -1,0 +1,241 @@
+/*
+ * disco_b200.h — C-ABI of the B200 (sm_100a) displacement backend for DISCO.
+ *
+ * Every entry point takes plain pointers and sizes and returns a status code
+ * (DISCO_OK on success); no C++ or torch type crosses this boundary.  The C++
+ * shim `backend_shim.cpp` re-exposes the four GPU functions of the reference's
+ * backend interface (Code/backend.hpp:57-62) on top of these calls, so the
+ * reference driver (Code/main.cpp:713-730) selects this backend unchanged.
+ *
+ * Conventions taken from the reference:
+ *   - atoms are SoA doubles, displacements are ACCUMULATED (+=) into arrays
+ *     the caller zeroed (Code/backend.hpp:28, Code/backend_cpu.cpp:57-59);
+ *   - a line loop's Burgers vector is (phys.bx*mx, phys.by*my, phys.bz*mz)
+ *     (Code/backend_cpu.cpp:44-45);
+ *   - the box is orthorhombic with lengths box[0..2]; image (i, j, k) moves the
+ *     atom by -(i*box[0], j*box[1], k*box[2]) (Code/backend_cpu.cpp:51-54).
+ * Errors are status codes; disco_b200_last_error() gives the message.  The
+ * reference prints and exits instead (Code/backend_cuda.cu:45-53); the shim
+ * maps a non-zero status to exactly that.
+ */
+#ifndef DISCO_B200_H
+#define DISCO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------- */
+#define DISCO_OK        0
+#define DISCO_EINVAL    1   /* bad argument: null pointer, negative size, bad loop  */
+#define DISCO_ENODEV    2   /* no CUDA device usable by this process               */
+#define DISCO_ECUDA     3   /* a CUDA runtime call or a kernel launch failed       */
+#define DISCO_ENOMEM    4   /* a device or pinned-host allocation failed           */
+#define DISCO_ELIMIT    5   /* a size is above a compiled-in or caller capacity    */
+#define DISCO_ETIMEOUT  6   /* a bounded device-side wait gave up                  */
+#define DISCO_EPLANES   7   /* |b.n| is not a whole number of plane spacings
+                               (the reference aborts: Code/prismatic.cpp:50-56)   */
+
+/* ---- precision of the displacement sum ------------------------------------- */
+#define DISCO_FP64      0   /* plain drop-in: FP64 throughout                      */
+#define DISCO_FP32C     1   /* FP32 bulk on loop-centred coordinates, compensated
+                               sums over images and loops, FP64 image offsets     */
+
+/* ---- loop shapes (Code/loop.hpp:13) ----------------------------------------- */
+#define DISCO_SHAPE_CIRCLE         0
+#define DISCO_SHAPE_RECTANGLE      1
+#define DISCO_SHAPE_PARALLELOGRAM  2
+#define DISCO_SHAPE_POLYGON        3
+#define DISCO_MAX_POLY            32   /* polygon vertices per slab loop            */
+
+/* ---- matter type of a slab loop (Code/prismatic.hpp:40) -------------------- */
+#define DISCO_MATTER_NONE          0
+#define DISCO_MATTER_VACANCY       1
+#define DISCO_MATTER_INTERSTITIAL  2
+
+/* Atom positions (read) and displacements (accumulated).  Code/backend.hpp:29-33.
+ * Host pointers for disco_b200_displace, device pointers for
+ * disco_b200_plan_execute. */
+typedef struct {
+    const double *x, *y, *z;
+    double *ux, *uy, *uz;
+    int64_t n;
+} disco_atoms;
+
+/* Loop physics, field for field the reference's LoopPhys (Code/kroupa.hpp:28-36):
+ * b = |b| per axis, m and n unit vectors, dS the loopon area. */
+typedef struct {
+    double bx, by, bz;
+    double mx, my, mz;
+    double nx, ny, nz;
+    double dS;
+} disco_loop_phys;
+
+/* One loop as the backend sees it: Code/backend.hpp:20-26 (LoopData).
+ * line != 0: closed polyline vx/vy/vz[0..n_vertices-1] (counter-clockwise about
+ * n, last vertex joined to the first) with fan apex (cx, cy, cz);
+ * line == 0: loopon positions x/y/z[0..n_loopons-1].  Host pointers. */
+typedef struct {
+    const double *x, *y, *z;
+    int32_t n_loopons;
+    int32_t line;
+    disco_loop_phys phys;
+    const double *vx, *vy, *vz;
+    int32_t n_vertices;
+    int32_t reserved;
+    double cx, cy, cz;
+} disco_loop;
+
+/* Options of the displacement sum.  The reference's GpuOptions
+ * (Code/backend.hpp:53-56) holds fp32 and chunkPairs; images and nu are fixed
+ * there at 1 and 0.35 (Code/backend_cpu.cpp:51-53, Code/kroupa.hpp:24) and are
+ * parameters here.  Fill with disco_b200_options_default() first. */
+typedef struct {
+    int32_t precision;     /* DISCO_FP64 or DISCO_FP32C                            */
+    int32_t images;        /* image range: -images..+images per axis, 0..8         */
+    double  nu;            /* Poisson ratio, in (-1, 0.5)                          */
+    double  chunk_pairs;   /* accepted for GpuOptions compatibility; B200 needs no
+                              watchdog chunking, so it is ignored                  */
+    int32_t atoms_per_thread;  /* 0 = automatic                                    */
+    int32_t threads_per_block; /* 0 = automatic                                    */
+    int32_t image_split;       /* lanes sharing one atom's images (1..32, power of
+                                  two); 0 = automatic                              */
+    int32_t verbose;           /* print the reference's per-loop banner lines      */
+} disco_options;
+
+/* Phase timings, seconds: Code/backend.hpp:36-39 (BackendTiming).
+ * loop_sec: caller array of nloops entries, or NULL.  All loops run in one
+ * launch here, so loop_sec[l] is the kernel time apportioned by loop l's share
+ * of the evaluations (never zero for a non-empty loop, as the reference's
+ * pair-rate report divides by it: Code/main.cpp:962). */
+typedef struct {
+    double upload, kernels, download;
+    double *loop_sec;
+} disco_timing;
+
+/* Work counts of a plan. */
+typedef struct {
+    int64_t n_loops, n_line_loops, n_loopon_loops;
+    int64_t n_segments, n_loopons, n_images;
+    double  evals_per_atom;   /* (segments + loopons) x images                     */
+} disco_plan_stats;
+
+typedef struct disco_plan disco_plan;
+
+/* ---- device queries ---------------------------------------------------------- */
+
+/* 1 if a CUDA device is usable; replaces gpuAvailable() (Code/backend.hpp:58). */
+int disco_b200_available(void);
+
+/* Writes the "--- GPU: <name> ---" banner of printGpuInfo() (Code/backend.hpp:59,
+ * Code/backend_cuda.cu:543-553) into buf.  DISCO_ENODEV without a device. */
+int disco_b200_device_info(char *buf, size_t len);
+
+/* 1: this build has the FP64 line kernel; replaces gpuLineFp64()
+ * (Code/backend.hpp:60).  Always 1 on sm_100a. */
+int disco_b200_line_fp64(void);
+
+void disco_b200_options_default(disco_options *opt);
+
+/* Message of the last failing call on this thread (empty if none). */
+const char *disco_b200_last_error(void);
+const char *disco_b200_strerror(int status);
+
+/* ---- displacement sum ---------------------------------------------------------- */
+
+/* Host buffers in, host buffers out: uploads the atoms, sums every loop over
+ * every image in one launch, adds the result into atoms->ux/uy/uz.  Replaces
+ * kroupaGPU (Code/backend.hpp:61-62, Code/backend_cuda.cu:568-722). */
+int disco_b200_displace(const disco_atoms *atoms, const disco_loop *loops, int32_t nloops,
+                        const double box[3], const disco_options *opt, disco_timing *timing);
+
+/* Resident form: the loop tables are built and uploaded once by plan_create;
+ * plan_execute adds the field of every loop into DEVICE arrays on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) without any host copy. */
+int disco_b200_plan_create(const disco_loop *loops, int32_t nloops, const double box[3],
+                           const disco_options *opt, int64_t max_atoms, disco_plan **out);
+int disco_b200_plan_execute(disco_plan *plan, const disco_atoms *device_atoms, void *stream);
+int disco_b200_plan_stats(const disco_plan *plan, disco_plan_stats *stats);
+/* Waits for `stream` and reports what the plan's kernels recorded on the
+ * device since the last call (DISCO_ETIMEOUT if a bounded wait gave up). */
+int disco_b200_plan_sync(disco_plan *plan, void *stream);
+int disco_b200_plan_destroy(disco_plan *plan);
+
+/* ---- prismatic loops: slab selection and stream compaction ------------------------ */
+
+/* One loop of the matter step.  Geometry as in the reference's loop class
+ * (Code/loop.hpp:19-45): centre c on a mid-plane, unit m and n, |b| = bmag,
+ * in-plane grid axes u, v (oblique for a parallelogram), shape parameters, and
+ * for a polygon the vertex, inner-vertex and inward-normal arrays (pu..nv). */
+typedef struct {
+    double c[3], m[3], n[3];
+    double bmag;
+    double u[3], v[3];
+    double spacing;             /* d: atomic-plane spacing of the n family            */
+    int32_t shape;              /* DISCO_SHAPE_*                                       */
+    int32_t n_poly;             /* polygon vertex count, <= DISCO_MAX_POLY             */
+    double radius, half_m, half_p, r_corner;
+    double pu[DISCO_MAX_POLY], pv[DISCO_MAX_POLY];
+    double qu[DISCO_MAX_POLY], qv[DISCO_MAX_POLY];
+    double nu[DISCO_MAX_POLY], nv[DISCO_MAX_POLY];
+    double shift_pos[3];        /* copy shift of a side +1 atom (interstitial): +b,
+                                   plus the Shockley shift of a Frank loop
+                                   (Code/main.cpp:630-650)                           */
+    double shift_neg[3];        /* copy shift of a side -1 atom                        */
+    int32_t apply;              /* 0: "Matter: none", displacement only (main.cpp:593) */
+    int32_t reserved;
+} disco_slab_loop;
+
+/* Per-loop result, the scalar part of SlabResult (Code/prismatic.hpp:47-55). */
+typedef struct {
+    int32_t type;               /* DISCO_MATTER_*                                      */
+    int32_t planes;             /* k                                                   */
+    double  height, spacing;    /* |b.n|, d                                            */
+    double  b[3];               /* |b| m                                               */
+    int64_t offset, count;      /* this loop's entries in slab_atoms / slab_side       */
+} disco_slab_info;
+
+/* An interstitial copy after compaction: source atom (new index) and shift. */
+typedef struct {
+    int32_t atom;
+    int32_t reserved;
+    double  shift[3];
+} disco_copy;
+
+/* Matter step of Code/main.cpp:586-687 on the GPU, host buffers.
+ * For every loop with b.n != 0 and apply != 0: the slab atoms of prismaticSlab
+ * (Code/prismatic.cpp:36-74), ascending, with their side; vacancy slabs are
+ * removed and interstitial slabs give copies (loop order, then slab order).
+ * Outputs: survivors x_out/y_out/z_out[0..counts[0]) in original order,
+ * new_index[n] (-1 for a removed atom), info[nloops], slab_atoms/slab_side
+ * (capacity slab_capacity, entries of loop l at info[l].offset), copies
+ * (capacity copy_capacity) with their source renumbered and copies of removed
+ * atoms dropped.  counts = {survivors, slab entries, copies}; when a capacity
+ * is too small the call returns DISCO_ELIMIT with counts holding the sizes
+ * needed.  Selection is bit-exact with the reference's FP64 predicate. */
+int disco_b200_prismatic(const double *x, const double *y, const double *z, int64_t n,
+                         const disco_slab_loop *loops, int32_t nloops, const double box[3],
+                         double *x_out, double *y_out, double *z_out, int32_t *new_index,
+                         disco_slab_info *info,
+                         int32_t *slab_atoms, int8_t *slab_side, int64_t slab_capacity,
+                         disco_copy *copies, int64_t copy_capacity,
+                         int64_t counts[3]);
+
+/* Code/main.cpp:733-743 and 797-818 fused: appends the copies (position of the
+ * source, displacement u(source) + shift) after the n atoms, then writes the
+ * wrapped final positions r = x + u, folded once into [-L/2, L/2] and shifted
+ * by +L/2.  Output arrays hold n + ncopies entries; ux/uy/uz_out may be NULL. */
+int disco_b200_finalize(const double *x, const double *y, const double *z,
+                        const double *ux, const double *uy, const double *uz, int64_t n,
+                        const disco_copy *copies, int64_t ncopies, const double box[3],
+                        double *fx, double *fy, double *fz,
+                        double *ux_out, double *uy_out, double *uz_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DISCO_B200_H */

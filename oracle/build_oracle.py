@@ -1,0 +1,81 @@
+"""Build recipe of the oracle (test infrastructure only).
+
+Three shared libraries, all host code:
+
+  oracle/_build/libdisco_oracle.so        the CPU restatement, compiled with the
+                                           reference's flags (-O3 -fopenmp, FMA
+                                           contraction left on, Code/Makefile:66)
+  oracle/_build/libdisco_oracle_nofma.so  the same with -ffp-contract=off: the
+                                           pinned build the atom-set checks use
+  oracle/_ref/libdisco_ref.so             the reference's own backend_cpu.cpp,
+                                           loop.cpp and prismatic.cpp compiled in
+                                           place from the reference tree, plus
+                                           oracle/ref_harness.cpp; built only where
+                                           the reference tree exists
+  oracle/_ref/libdisco_ref_nofma.so       the same with -ffp-contract=off
+
+GCC contracts a*b+c into FMAs where it sees fit, and it does not contract the
+reference and the restatement identically (the reference folds nu = 0.35 at
+compile time).  The contract-off builds of both are bit-identical; the
+difference between the two default builds is the rounding floor of the
+comparison, reported by the tests.
+
+`-march=x86-64-v3` replaces the reference's `-march=native` so that the
+libraries built here also run on the GPU host (AVX2 + FMA); both the reference
+and the restatement get the same flags, which is what bit-identity needs.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+REF_CODE = os.environ.get("DISCO_REFERENCE_CODE", "/root/reference/Code")
+
+CXX = os.environ.get("DISCO_CXX", "g++")
+BASE = ["-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared"]
+
+ORACLE_SO = os.path.join(HERE, "_build", "libdisco_oracle.so")
+ORACLE_NOFMA_SO = os.path.join(HERE, "_build", "libdisco_oracle_nofma.so")
+REF_SO = os.path.join(HERE, "_ref", "libdisco_ref.so")
+REF_NOFMA_SO = os.path.join(HERE, "_ref", "libdisco_ref_nofma.so")
+
+
+def _stale(out, deps):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(force=False, verbose=True):
+    os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
+    src = os.path.join(HERE, "disco_oracle.cpp")
+    hdr = os.path.join(REPO, "include", "disco_b200.h")
+    if force or _stale(ORACLE_SO, [src, hdr, __file__]):
+        _run([CXX, "-std=c++17", *BASE, src, "-o", ORACLE_SO])
+    if force or _stale(ORACLE_NOFMA_SO, [src, hdr, __file__]):
+        _run([CXX, "-std=c++17", *BASE, "-ffp-contract=off", src, "-o", ORACLE_NOFMA_SO])
+    if os.path.isdir(REF_CODE):
+        os.makedirs(os.path.join(HERE, "_ref"), exist_ok=True)
+        harness = os.path.join(HERE, "ref_harness.cpp")
+        ref_srcs = [os.path.join(REF_CODE, f) for f in ("backend_cpu.cpp", "loop.cpp", "prismatic.cpp")]
+        ref_hdrs = [os.path.join(REF_CODE, f) for f in
+                    ("backend.hpp", "barnett.hpp", "kroupa.hpp", "lattice.hpp", "loop.hpp", "prismatic.hpp")]
+        deps = [harness, hdr, __file__, *ref_srcs, *ref_hdrs]
+        if force or _stale(REF_SO, deps):
+            _run([CXX, "-std=c++14", *BASE, "-I", REF_CODE, harness, *ref_srcs, "-o", REF_SO])
+        if force or _stale(REF_NOFMA_SO, deps):
+            _run([CXX, "-std=c++14", *BASE, "-ffp-contract=off", "-I", REF_CODE, harness, *ref_srcs,
+                  "-o", REF_NOFMA_SO])
+    elif verbose:
+        print(f"reference tree {REF_CODE} absent: oracle/_ref not rebuilt", flush=True)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

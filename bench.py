@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--image-split", type=int, default=0)
+    p.add_argument("--images", type=int, default=None,
+                   help="override the workload's image range (profiling of small cases)")
     return p.parse_args()
 
 
@@ -64,9 +66,12 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", 0))
 
 
-def build_workload(name):
+def build_workload(name, images=None):
     from disco_b200 import workloads as W
-    return W.FULL[name]()
+    w = W.FULL[name]()
+    if images is not None:
+        w.images = images
+    return w
 
 
 def flop_per_eval(w):
@@ -193,7 +198,7 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    w = build_workload(args.config)
+    w = build_workload(args.config, args.images)
     import oracle as O
     threads = os.cpu_count() or 1
     ref_ok = w.images == 1 and O.have_ref()
@@ -248,7 +253,7 @@ def run_ours(args):
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    w = build_workload(args.config)
+    w = build_workload(args.config, args.images)
     prec = C.DISCO_FP32C if args.precision == "fp32c" else C.DISCO_FP64
     n = w.n
     plan = B.Plan(w.loops, w.box, precision=prec, images=w.images, nu=w.nu,

@@ -51,7 +51,7 @@ def build(force=False, verbose=True, ptxas_info=False):
         [os.path.join(INC, "disco_b200.h"), __file__]
     if force or _stale(LIB_CUDA, deps):
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-shared",
-               "-Xcompiler", "-fPIC,-O3", "-I", INC, *srcs, "-o", LIB_CUDA]
+               "-Xcompiler", "-fPIC,-O3,-ffp-contract=off", "-I", INC, *srcs, "-o", LIB_CUDA]
         if ptxas_info:
             cmd.insert(1, "-Xptxas=-v")
         _run(cmd, verbose)

@@ -11,6 +11,7 @@
 
 #include <cuda_runtime.h>
 
+#include "common.cuh"
 #include "field.cuh"
 
 namespace disco {
@@ -88,6 +89,8 @@ double now_s()
 }
 
 } // namespace
+
+void disco::set_last_error(const std::string& msg) { g_last_error = msg; }
 
 extern "C" {
 

@@ -3,11 +3,15 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "../../include/disco_b200.h"
 
 namespace disco {
+
+// Message returned by disco_b200_last_error() for the calling thread.
+void set_last_error(const std::string& msg);
 
 // A bounded wait gives up after this many nanoseconds of %globaltimer.  A stage
 // copy of a few hundred KB completes in microseconds; the bound only exists so

@@ -46,7 +46,8 @@ class DiscoLoop(Structure):
 class DiscoOptions(Structure):
     _fields_ = [("precision", c_int32), ("images", c_int32), ("nu", c_double),
                 ("chunk_pairs", c_double), ("atoms_per_thread", c_int32),
-                ("threads_per_block", c_int32), ("image_split", c_int32), ("verbose", c_int32)]
+                ("threads_per_block", c_int32), ("image_split", c_int32), ("verbose", c_int32),
+                ("near_plane", c_double), ("near_rim", c_double)]
 
 
 class DiscoTiming(Structure):

@@ -118,7 +118,8 @@ def loop_array(loops):
     return arr, keep
 
 
-def options(precision=C.DISCO_FP64, images=1, nu=0.35, image_split=0, verbose=0):
+def options(precision=C.DISCO_FP64, images=1, nu=0.35, image_split=0, verbose=0, near_plane=0.0,
+            near_rim=0.0):
     lib = C.cuda_lib()
     o = C.DiscoOptions()
     lib.disco_b200_options_default(ctypes.byref(o))
@@ -127,6 +128,8 @@ def options(precision=C.DISCO_FP64, images=1, nu=0.35, image_split=0, verbose=0)
     o.nu = nu
     o.image_split = image_split
     o.verbose = verbose
+    o.near_plane = near_plane
+    o.near_rim = near_rim
     return o
 
 
@@ -153,13 +156,14 @@ def gpu_line_fp64():
 
 
 def kroupa_gpu(atoms, loops, dx, dy, dz, opt=None, t=None, *, images=1, nu=0.35, image_split=0,
-               verbose=0):
+               verbose=0, near_plane=0.0, near_rim=0.0):
     """kroupaGPU (Code/backend.hpp:61-62): adds the field of every loop over its
     periodic images into atoms.ux/uy/uz.  images and nu default to the
     reference's fixed values (+-1, 0.35).  Raises DiscoError on failure."""
     opt = opt or GpuOptions()
     lib = C.cuda_lib()
-    o = options(C.DISCO_FP32C if opt.fp32 else C.DISCO_FP64, images, nu, image_split, verbose)
+    o = options(C.DISCO_FP32C if opt.fp32 else C.DISCO_FP64, images, nu, image_split, verbose,
+                near_plane, near_rim)
     o.chunk_pairs = opt.chunkPairs
     for name in ("x", "y", "z", "ux", "uy", "uz"):
         a = getattr(atoms, name)

@@ -24,7 +24,7 @@ CXX = os.environ.get("DISCO_CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CUDA_SOURCES = ["field.cu", "field_fp32.cu", "prismatic.cu", "capi.cu"]
-CUDA_HEADERS = ["common.cuh", "field.cuh"]
+CUDA_HEADERS = ["common.cuh", "field.cuh", "field_device.cuh"]
 
 LIB_CUDA = os.path.join(LIB, "libdisco_b200.so")
 LIB_GEOM = os.path.join(LIB, "libdisco_geom.so")

@@ -65,6 +65,8 @@ int check_options(const disco_options& o)
         return fail(DISCO_EINVAL, "precision must be DISCO_FP64 or DISCO_FP32C");
     if (o.images < 0 || o.images > 8) return fail(DISCO_EINVAL, "images must be in 0..8");
     if (!(o.nu > -1.0 && o.nu < 0.5)) return fail(DISCO_EINVAL, "nu must be in (-1, 0.5)");
+    if (!(o.near_plane >= 0.0) || !(o.near_rim >= 0.0))
+        return fail(DISCO_EINVAL, "near_plane and near_rim must be >= 0");
     if (o.image_split != 0 && (o.image_split < 1 || o.image_split > 32 ||
                                (o.image_split & (o.image_split - 1))))
         return fail(DISCO_EINVAL, "image_split must be 0 or a power of two up to 32");
@@ -235,6 +237,12 @@ int disco_b200_plan_execute(disco_plan* p, const disco_atoms* a, void* stream)
         fa.cK = c3;
         fa.c2 = 1.0 - 2.0 * p->opt.nu;                              // Code/kroupa.hpp:66
         fa.status = p->d_status;
+        fa.near_h = (float)p->opt.near_plane;
+        fa.near_r = (float)p->opt.near_rim;
+        if (T.fp32 && k == 0 && T.aux_pieces) {
+            fa.pieces64 = reinterpret_cast<const disco::LinePiece*>(p->d_table[k] + T.aux_pieces);
+            fa.segs64 = reinterpret_cast<const disco::LineSeg*>(p->d_table[k] + T.aux_segs);
+        }
         std::string err;
         const int kind = k == 0 ? disco::kLineKind : disco::kLooponKind;
         const int st = T.fp32

@@ -56,15 +56,23 @@ struct alignas(16) LooponRec {
 static_assert(sizeof(LooponPiece) == 112 && sizeof(LooponRec) == 48, "loopon table layout");
 
 // ---- FP32 compensated forms -------------------------------------------------------
+// Bulk arithmetic in FP32 on coordinates relative to the loop centre; the
+// centre and the image offsets stay FP64.  A line piece also carries what the
+// near-cut test needs (plane normal, largest vertex radius) and the index of
+// the same piece in the FP64 table, which is evaluated instead for an atom
+// within a few A of the loop's plane disc.
 struct alignas(16) LinePieceF {
-    double cx, cy, cz;    // loop centre (FP64): atoms enter relative to it
-    float ax, ay, az;     // start vertex relative to the centre
-    float bx, by, bz;     // Burgers vector
+    double cx, cy, cz;       // loop centre (FP64)
+    float ax, ay, az;        // start vertex - centre
+    float bx, by, bz;        // Burgers vector
+    float nx, ny, nz;        // unit normal of the loop plane
+    float rmax;              // largest |vertex - centre| of the loop
     int32_t nseg, rec;
-    int32_t pad0, pad1, pad2;   // 24 + 24 + 20 -> 80 B
+    int32_t piece64;         // this piece in the FP64 table
+    int32_t pad;             // 80 B
 };
 struct alignas(16) LineSegF {
-    float vx, vy, vz, len;   // end vertex relative to the centre, length
+    float vx, vy, vz, len;   // end vertex - centre, length
     float tx, ty, tz;        // unit tangent
     float wx, wy, wz;        // b x t
     float pad0, pad1;        // 48 B
@@ -76,8 +84,8 @@ struct alignas(16) LooponPieceF {
     float fbx, fby, fbz;    // -k1 dS b
     float mx, my, mz, nx, ny, nz;
     float b_n;
-    int32_t n, rec;         // 24 + 48 + 8 = 80 B
-    int32_t pad0, pad1;
+    int32_t n, rec;
+    int32_t pad0, pad1;     // 80 B
 };
 struct alignas(16) LooponRecF {
     float x, y, z, ml;      // loopon - c, m . (loopon - c)
@@ -106,6 +114,11 @@ struct FieldArgs {
     double cJ, cK;            // line: c3 - 1/(4 pi), c3 = 1 / (8 pi (1 - nu))
     double c2;                // loopon: 1 - 2 nu
     int* status;
+    // FP32 line form: the FP64 pieces (flat, rec = global segment index) for
+    // atoms near a loop's cut, and the near-cut distances
+    const LinePiece* pieces64;
+    const LineSeg* segs64;
+    float near_h, near_r;
 };
 
 // Host-side table: bytes + chunk list, built once per plan.
@@ -118,6 +131,9 @@ struct HostTable {
     bool resident = false;
     std::vector<double> loop_evals;   // evaluations per atom per image, per input loop
     int64_t n_segments = 0, n_loopons = 0;
+    // FP32 line tables: byte offsets of the flat FP64 pieces and segments
+    // appended after the chunks (0 when absent)
+    uint64_t aux_pieces = 0, aux_segs = 0;
 };
 
 // Builds the table of the loops of one kind (kLineKind: loops with line != 0,

@@ -1,0 +1,339 @@
+// Device building blocks of the displacement kernels (FP64 piece fields,
+// image enumeration) and the host helper that packs pieces into chunks.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "field.cuh"
+
+namespace disco {
+
+constexpr int kThreads = 256;
+constexpr int kMaxLinePiece = 256;         // segments per piece
+constexpr int kMaxLooponPiece = 960;       // loopons per piece (fits a 48 KB stage)
+constexpr uint32_t kResidentMax = 110u * 1024u;
+constexpr uint32_t kStageMax = 48u * 1024u;
+constexpr uint32_t kSmemHeader = 128;      // mbarriers at the start of shared memory
+
+__device__ __forceinline__ void image_shift(int img, int images, double Lx, double Ly, double Lz,
+                                            double& sx, double& sy, double& sz)
+{
+    const int W = 2 * images + 1;
+    const int ii = img / (W * W) - images;
+    const int r = img % (W * W);
+    const int jj = r / W - images;
+    const int kk = r % W - images;
+    sx = Lx * ii;
+    sy = Ly * jj;
+    sz = Lz * kk;
+}
+
+// Field at P (an atom moved by minus an image shift) of one line piece.
+// Follows Code/barnett.hpp:55-106 term by term (see the file header for the
+// reformulations); adds b Omega/(4 pi) + the line terms to (ux, uy, uz).
+__device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineSeg* seg,
+                                                double Px, double Py, double Pz, double cJ, double cK,
+                                                double& ux, double& uy, double& uz)
+{
+    // unit vector from P to the fan apex
+    const double r1x = pc.cx - Px, r1y = pc.cy - Py, r1z = pc.cz - Pz;
+    const double il1 = rsqrt(r1x * r1x + r1y * r1y + r1z * r1z);
+    const double ex = r1x * il1, ey = r1y * il1, ez = r1z * il1;
+
+    // vertex A (start of the current segment) relative to P
+    double ax = pc.ax - Px, ay = pc.ay - Py, az = pc.az - Pz;
+    double ila = rsqrt(ax * ax + ay * ay + az * az);
+    double la = (ax * ax + ay * ay + az * az) * ila;
+    double hax = ax * ila, hay = ay * ila, haz = az * ila;
+    double ca = ex * hax + ey * hay + ez * haz;                 // e . a-hat
+    double qx = ey * haz - ez * hay, qy = ez * hax - ex * haz, qz = ex * hay - ey * hax;   // e x a-hat
+
+    double zr = 1.0, zi = 0.0;                                   // running product
+    double lx = 0.0, ly = 0.0, lz = 0.0;
+    const int nseg = pc.nseg;
+    for (int k = 0; k < nseg; ++k) {
+        const LineSeg s = seg[k];
+        const double bx = s.vx - Px, by = s.vy - Py, bz = s.vz - Pz;
+        const double lb2 = bx * bx + by * by + bz * bz;
+        const double ilb = rsqrt(lb2);
+        const double lb = lb2 * ilb;
+        const double hbx = bx * ilb, hby = by * ilb, hbz = bz * ilb;
+        const double cb = ex * hbx + ey * hby + ez * hbz;
+
+        // solid angle of triangle (apex, A, B): tan(Omega/2) = num / den on unit
+        // vectors (Code/barnett.hpp:69-72 divided by l1 la lb > 0)
+        const double den = 1.0 + ca + cb + (hax * hbx + hay * hby + haz * hbz);
+        const double num = qx * hbx + qy * hby + qz * hbz;
+        const double nzr = zr * den - zi * num;
+        zi = zr * num + zi * den;
+        zr = nzr;
+
+        // segment A -> B (Code/barnett.hpp:75-100)
+        const double sA = ax * s.tx + ay * s.ty + az * s.tz;
+        const double sB = sA + s.len;
+        const double dx = ax - sA * s.tx, dy = ay - sA * s.ty, dz = az - sA * s.tz;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double dw = dx * s.wx + dy * s.wy + dz * s.wz;
+        const double sum = la + lb;
+        const double J0 = log((sum + s.len) / (sum - s.len));
+        const double g = sB * ilb - sA * ila;                   // d^2 K0
+        const double q = d2 > 0.0 ? dw / d2 : 0.0;
+        const double K1 = ila - ilb;
+        const double al = cK * q * g, be = cK * dw * K1, ga = cJ * J0;
+        lx += ga * s.wx - al * dx - be * s.tx;
+        ly += ga * s.wy - al * dy - be * s.ty;
+        lz += ga * s.wz - al * dz - be * s.tz;
+
+        ax = bx; ay = by; az = bz;
+        la = lb; ila = ilb;
+        hax = hbx; hay = hby; haz = hbz;
+        ca = cb;
+        qx = ey * hbz - ez * hby; qy = ez * hbx - ex * hbz; qz = ex * hby - ey * hbx;
+        if ((k & 63) == 63) {                                   // keep |z| near 1
+            const double sc = 1.0 / (fabs(zr) + fabs(zi));
+            zr *= sc; zi *= sc;
+        }
+    }
+    const double f = atan2(zi, zr) * (1.0 / 6.283185307179586476925286766559);   // Omega / (4 pi)
+    ux += pc.bx * f + lx;
+    uy += pc.by * f + ly;
+    uz += pc.bz * f + lz;
+}
+
+// Field at P (atom - reference point - image shift) of one loopon piece:
+// Code/kroupa.hpp:52-73 with 1/rho from one rsqrt and m.rho, n.rho from
+// per-loopon projections.
+__device__ __forceinline__ void loopon_piece_fp64(const LooponPiece& pc, const LooponRec* __restrict__ rec,
+                                                  double Px, double Py, double Pz, double c2,
+                                                  double& ux, double& uy, double& uz)
+{
+    const double mP = pc.mx * Px + pc.my * Py + pc.mz * Pz;
+    const double nP = pc.nx * Px + pc.ny * Py + pc.nz * Pz;
+    double dx = 0.0, dy = 0.0, dz = 0.0;
+    const int n = pc.n;
+    for (int k = 0; k < n; ++k) {
+        const LooponRec l = rec[k];
+        const double rx = Px - l.x, ry = Py - l.y, rz = Pz - l.z;
+        const double r2 = rx * rx + ry * ry + rz * rz;
+        const bool keep = r2 >= 1e-20;                           // rho >= 1e-10 (kroupa.hpp:55)
+        const double ir = rsqrt(keep ? r2 : 1.0);
+        const double ir2 = ir * ir;
+        const double mr = mP - l.ml, nr = nP - l.nl;
+        const double k2 = c2 * ir;
+        const double tail = 3.0 * mr * nr * (ir2 * ir);
+        const double fac = keep ? ir2 : 0.0;
+        const double ex = pc.nx * mr + pc.mx * nr - rx * pc.b_n;
+        const double ey = pc.ny * mr + pc.my * nr - ry * pc.b_n;
+        const double ez = pc.nz * mr + pc.mz * nr - rz * pc.b_n;
+        dx += fac * (pc.fbx * (k2 * ex + tail * rx));
+        dy += fac * (pc.fby * (k2 * ey + tail * ry));
+        dz += fac * (pc.fbz * (k2 * ez + tail * rz));
+    }
+    ux += dx; uy += dy; uz += dz;
+}
+
+// ---- the two FP64 policies ----------------------------------------------------------------
+
+struct AccF64 {
+    double x, y, z;
+    __device__ void clear() { x = y = z = 0.0; }
+    __device__ void total(double& ux, double& uy, double& uz) const { ux = x; uy = y; uz = z; }
+};
+
+struct LineFp64 {
+    using Acc = AccF64;
+    static constexpr int kMinBlocks = 2;
+    template <int S>
+    static __device__ __forceinline__ void chunk(const FieldArgs& a, const unsigned char* st, int npieces,
+                                                 int split, double px, double py, double pz, Acc& acc)
+    {
+        const LinePiece* pieces = reinterpret_cast<const LinePiece*>(st);
+        const LineSeg* recs = reinterpret_cast<const LineSeg*>(st + (size_t)npieces * sizeof(LinePiece));
+        for (int p = 0; p < npieces; ++p) {
+            const LinePiece& pc = pieces[p];
+            for (int img = split; img < a.nimg; img += S) {
+                double sx, sy, sz;
+                image_shift(img, a.images, a.Lx, a.Ly, a.Lz, sx, sy, sz);
+                line_piece_fp64(pc, recs + pc.rec, px - sx, py - sy, pz - sz, a.cJ, a.cK, acc.x, acc.y, acc.z);
+            }
+        }
+    }
+};
+
+struct LooponFp64 {
+    using Acc = AccF64;
+    static constexpr int kMinBlocks = 2;
+    template <int S>
+    static __device__ __forceinline__ void chunk(const FieldArgs& a, const unsigned char* st, int npieces,
+                                                 int split, double px, double py, double pz, Acc& acc)
+    {
+        const LooponPiece* pieces = reinterpret_cast<const LooponPiece*>(st);
+        const LooponRec* recs = reinterpret_cast<const LooponRec*>(st + (size_t)npieces * sizeof(LooponPiece));
+        for (int p = 0; p < npieces; ++p) {
+            const LooponPiece& pc = pieces[p];
+            const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
+            for (int img = split; img < a.nimg; img += S) {
+                double sx, sy, sz;
+                image_shift(img, a.images, a.Lx, a.Ly, a.Lz, sx, sy, sz);
+                loopon_piece_fp64(pc, recs + pc.rec, qx - sx, qy - sy, qz - sz, a.c2, acc.x, acc.y, acc.z);
+            }
+        }
+    }
+};
+
+// Persistent kernel: CTA b takes atom tiles b, b + grid, ...; for each tile it
+// walks the chunks of the table (staged in shared memory) and, per piece, the
+// images of its lane's share.
+template <class Policy, int S>
+__global__ void __launch_bounds__(kThreads, Policy::kMinBlocks) field_kernel(const FieldArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+    unsigned char* const stage0 = smem + kSmemHeader;
+    const int tid = threadIdx.x;
+    constexpr int kAtomsPerCta = kThreads / S;
+    const int64_t ntiles = (a.n + kAtomsPerCta - 1) / kAtomsPerCta;
+    if ((int64_t)blockIdx.x >= ntiles) return;
+    const int nch = a.nchunks;
+    const bool resident = a.resident != 0;
+    const int64_t my_tiles = (ntiles - 1 - (int64_t)blockIdx.x) / gridDim.x + 1;
+    const int64_t nunits = resident ? my_tiles : my_tiles * nch;
+
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int64_t u) {
+        const int ch = resident ? 0 : (int)(u % nch);
+        const int buf = resident ? 0 : (int)(u & 1);
+        const Chunk c = a.chunks[ch];
+        stage_load(stage0 + (size_t)buf * a.stage_bytes, a.table + c.offset, c.bytes, &bar[buf]);
+    };
+    if (tid == 0) {
+        issue(0);
+        if (!resident && nunits > 1) issue(1);
+    }
+
+    const int split = tid % S;
+    double px = 0.0, py = 0.0, pz = 0.0;
+    typename Policy::Acc acc;
+    int64_t atom = 0;
+    bool valid = false;
+    for (int64_t u = 0; u < nunits; ++u) {
+        const int64_t tk = resident ? u : u / nch;
+        const int ch = resident ? 0 : (int)(u % nch);
+        const int buf = resident ? 0 : (int)(u & 1);
+        if (ch == 0) {
+            const int64_t tile = (int64_t)blockIdx.x + tk * gridDim.x;
+            atom = tile * kAtomsPerCta + tid / S;
+            valid = atom < a.n;
+            const int64_t ia = valid ? atom : a.n - 1;
+            px = a.x[ia]; py = a.y[ia]; pz = a.z[ia];
+            acc.clear();
+        }
+        if (!resident || u == 0) {
+            const uint32_t parity = resident ? 0u : (uint32_t)((u >> 1) & 1);
+            const bool ok = mbar_wait_bounded(&bar[buf], parity);
+            if (__syncthreads_or(!ok)) {
+                // give up: record it, let the copies still in flight land, return
+                if (tid == 0) {
+                    report(a.status, DISCO_ETIMEOUT);
+                    mbar_wait_bounded(&bar[buf], parity);
+                    if (!resident && u + 1 < nunits)
+                        mbar_wait_bounded(&bar[buf ^ 1], (uint32_t)(((u + 1) >> 1) & 1));
+                }
+                __syncthreads();
+                return;
+            }
+        }
+        const unsigned char* st = stage0 + (size_t)buf * a.stage_bytes;
+        Policy::template chunk<S>(a, st, a.chunks[ch].npieces, split, px, py, pz, acc);
+        if (resident || ch == nch - 1) {
+            double ux, uy, uz;
+            acc.total(ux, uy, uz);
+#pragma unroll
+            for (int o = S / 2; o > 0; o >>= 1) {
+                ux += __shfl_xor_sync(0xffffffffu, ux, o);
+                uy += __shfl_xor_sync(0xffffffffu, uy, o);
+                uz += __shfl_xor_sync(0xffffffffu, uz, o);
+            }
+            if (valid && split == 0) {
+                a.ux[atom] += ux;
+                a.uy[atom] += uy;
+                a.uz[atom] += uz;
+            }
+        }
+        if (!resident) {
+            __syncthreads();                       // every warp is done with stage[buf]
+            if (tid == 0 && u + 2 < nunits) {
+                fence_proxy_async_smem();
+                issue(u + 2);
+            }
+        }
+    }
+}
+
+
+// ---- host: tables -----------------------------------------------------------------------
+
+template <class Piece, class Rec>
+struct PieceList {
+    std::vector<Piece> pieces;
+    std::vector<std::vector<Rec>> recs;
+};
+
+template <class Piece, class Rec>
+void pack_chunks(PieceList<Piece, Rec>& L, HostTable& T)
+{
+    size_t total = 0;
+    for (size_t i = 0; i < L.pieces.size(); ++i) total += sizeof(Piece) + L.recs[i].size() * sizeof(Rec);
+    const uint32_t cap = total <= kResidentMax ? kResidentMax : kStageMax;
+    T.resident = total <= kResidentMax;
+    T.bytes.clear();
+    T.chunks.clear();
+    size_t i = 0;
+    uint32_t max_bytes = 16;
+    while (i < L.pieces.size()) {
+        // the longest run of pieces that fits in one stage
+        size_t j = i, bytes = 0;
+        while (j < L.pieces.size()) {
+            const size_t add = sizeof(Piece) + L.recs[j].size() * sizeof(Rec);
+            if (j > i && bytes + add > cap) break;
+            bytes += add;
+            ++j;
+        }
+        Chunk c;
+        c.offset = T.bytes.size();
+        c.bytes = (uint32_t)((bytes + 15) & ~size_t(15));
+        c.npieces = (int32_t)(j - i);
+        std::vector<unsigned char> blob(c.bytes, 0);
+        int32_t rec = 0;
+        for (size_t k = i; k < j; ++k) {
+            Piece p = L.pieces[k];
+            p.rec = rec;
+            std::memcpy(blob.data() + (k - i) * sizeof(Piece), &p, sizeof(Piece));
+            rec += (int32_t)L.recs[k].size();
+        }
+        size_t off = (j - i) * sizeof(Piece);
+        for (size_t k = i; k < j; ++k) {
+            std::memcpy(blob.data() + off, L.recs[k].data(), L.recs[k].size() * sizeof(Rec));
+            off += L.recs[k].size() * sizeof(Rec);
+        }
+        T.bytes.insert(T.bytes.end(), blob.begin(), blob.end());
+        T.chunks.push_back(c);
+        max_bytes = std::max(max_bytes, c.bytes);
+        i = j;
+    }
+    if (T.chunks.size() <= 1) T.resident = true;
+    T.stage_bytes = max_bytes;
+}
+
+
+
+} // namespace disco

@@ -104,6 +104,11 @@ typedef struct {
     int32_t image_split;       /* lanes sharing one atom's images (1..32, power of
                                   two); 0 = automatic                              */
     int32_t verbose;           /* print the reference's per-loop banner lines      */
+    double  near_plane;        /* DISCO_FP32C line method: an (atom, loop image)
+                                  within near_plane A of the loop plane and within
+                                  near_rim A beyond the loop's largest vertex radius
+                                  is evaluated in FP64; 0 = defaults (3 A, 3 A)   */
+    double  near_rim;
 } disco_options;
 
 /* Phase timings, seconds: Code/backend.hpp:36-39 (BackendTiming).

@@ -1,0 +1,62 @@
+"""The FP32 compensated form (DISCO_FP32C) against the FP64 oracle.
+
+Budget of the form: max |du| <= 1e-3 A; the tests hold it to 2e-5 A (the
+reference's own --fp32 line kernel reaches < 3e-5 A, loopons < 5e-6 A:
+docs/validation.md:161-165).  The near-cut FP64 pass is checked by moving its
+threshold: everything near (all FP64) must reproduce the FP64 kernel, nothing
+near must still be within budget on atoms away from the cut."""
+import numpy as np
+import pytest
+
+import oracle as O
+from disco_b200 import backend as B
+from disco_b200 import workloads as W
+from disco_b200.backend import AtomArrays, GpuOptions
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(w, fp32=True, atoms=None, **kw):
+    x, y, z = (w.x, w.y, w.z) if atoms is None else atoms
+    a = AtomArrays.zeros_like_positions(x, y, z)
+    B.kroupa_gpu(a, w.loops, *w.box, GpuOptions(fp32=fp32), images=w.images, nu=w.nu, **kw)
+    return np.stack([a.ux, a.uy, a.uz], 1)
+
+
+def _oracle(w, atoms=None):
+    x, y, z = (w.x, w.y, w.z) if atoms is None else atoms
+    return np.stack(O.displace(x, y, z, w.loops, w.box, images=w.images, nu=w.nu), 1)
+
+
+@pytest.mark.parametrize("name", ["quadrupole_small", "fcc_small", "prismatic_small"])
+def test_fp32c_within_budget(name):
+    w = {"quadrupole_small": lambda: W.quadrupole(cells=12, radius=9.0, eps=0.0365),
+         "fcc_small": lambda: W.fcc_random(cells=14, n_circles=6, n_hex=3, n_rect=3, seed=5),
+         "prismatic_small": lambda: W.bcc_prismatic(cells=12, rmin=4.0, rmax=9.0)}[name]()
+    d = np.abs(_run(w) - _oracle(w))
+    assert d.max() <= 2e-5, d.max()
+
+
+def test_near_cut_pass_is_fp64():
+    """near_plane huge: every pair goes through the FP64 pass, which must agree
+    with the FP64 kernel to rounding; near_plane tiny: FP32 everywhere."""
+    w = W.quadrupole(cells=10, radius=8.0, eps=0.0365)
+    f64 = _run(w, fp32=False)
+    all_near = _run(w, near_plane=1e6, near_rim=1e6)
+    assert np.abs(all_near - f64).max() <= 1e-12
+    none_near = _run(w, near_plane=1e-30, near_rim=1e-30)
+    ref = _oracle(w)
+    assert np.abs(none_near - ref).max() <= 1e-4
+    default = _run(w)
+    assert np.abs(default - ref).max() <= np.abs(none_near - ref).max() + 1e-12
+
+
+@pytest.mark.parametrize("name", ["quadrupole", "fcc_random", "bcc_prismatic"])
+def test_fp32c_full_size_subsample(name):
+    w = W.FULL[name]()
+    rng = np.random.default_rng(23)
+    k = {"quadrupole": 400, "fcc_random": 96, "bcc_prismatic": 24}[name]
+    idx = np.sort(rng.choice(w.n, size=k, replace=False))
+    g = _run(w)
+    ref = _oracle(w, atoms=(w.x[idx], w.y[idx], w.z[idx]))
+    assert np.abs(g[idx] - ref).max() <= 2e-5

@@ -137,6 +137,10 @@ def cuda_lib():
              [c_void_p, c_void_p, c_void_p, c_int64, POINTER(DiscoSlabLoop), c_int32,
               POINTER(c_double), c_void_p, c_void_p, c_void_p, c_void_p, POINTER(DiscoSlabInfo),
               c_void_p, c_void_p, c_int64, POINTER(DiscoCopy), c_int64, POINTER(c_int64)])
+        _sig(lib, "disco_b200_prismatic_noalloc", c_int,
+             [c_void_p, c_void_p, c_void_p, c_int64, POINTER(DiscoSlabLoop), c_int32,
+              POINTER(c_double), c_void_p, c_void_p, c_void_p, c_void_p, POINTER(DiscoSlabInfo),
+              c_void_p, c_void_p, c_int64, c_void_p, c_int64, POINTER(c_int64), c_void_p])
         _sig(lib, "disco_b200_finalize", c_int,
              [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
               POINTER(DiscoCopy), c_int64, POINTER(c_double), c_void_p, c_void_p, c_void_p,

@@ -39,11 +39,18 @@ struct disco_plan {
 
 namespace {
 
-thread_local std::string g_last_error;
+// Last error message of the calling thread: a fixed buffer, so that setting it
+// never allocates.
+thread_local char g_last_error[512];
+
+void store_error(const char* msg)
+{
+    std::snprintf(g_last_error, sizeof(g_last_error), "%s", msg);
+}
 
 int fail(int code, const std::string& msg)
 {
-    g_last_error = msg;
+    store_error(msg.c_str());
     return code;
 }
 
@@ -92,11 +99,12 @@ double now_s()
 
 } // namespace
 
-void disco::set_last_error(const std::string& msg) { g_last_error = msg; }
+void disco::set_last_error(const std::string& msg) { store_error(msg.c_str()); }
+void disco::set_last_error(const char* msg) { store_error(msg); }
 
 extern "C" {
 
-const char* disco_b200_last_error(void) { return g_last_error.c_str(); }
+const char* disco_b200_last_error(void) { return g_last_error; }
 
 const char* disco_b200_strerror(int s)
 {
@@ -335,7 +343,7 @@ int disco_b200_displace(const disco_atoms* atoms, const disco_loop* loops, int32
     e = cudaEventRecord(ev[1], s);
     if (e != cudaSuccess) { cleanup(); return cuda_fail(e, "event"); }
     st = disco_b200_plan_sync(plan, s);
-    if (st) { std::string m = g_last_error; cleanup(); return fail(st, m); }
+    if (st) { std::string m = g_last_error; cleanup(); return fail(st, m); }  // keep the kernel's message
     float ms = 0.f;
     cudaEventElapsedTime(&ms, ev[0], ev[1]);
     const double t2 = now_s();

@@ -10,8 +10,10 @@
 
 namespace disco {
 
-// Message returned by disco_b200_last_error() for the calling thread.
+// Message returned by disco_b200_last_error() for the calling thread (stored
+// in a fixed per-thread buffer; the const char* form never allocates).
 void set_last_error(const std::string& msg);
+void set_last_error(const char* msg);
 
 // A bounded wait gives up after this many nanoseconds of %globaltimer.  A stage
 // copy of a few hundred KB completes in microseconds; the bound only exists so

@@ -21,6 +21,7 @@
 // slab order, drops those of removed atoms and renumbers their sources.
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -400,46 +401,61 @@ int efail(int code, const std::string& msg)
     return code;
 }
 
-// Active loops in caller order, with their SlabResult scalars (prismatic.cpp:42-57).
+// One loop's SlabResult scalars (Code/prismatic.cpp:42-57) and, when it is
+// active (b.n != 0 and apply), its device record.  Never allocates.
+int slab_loop_record(const disco_slab_loop& g, int l, disco_slab_info& in, disco::SlabLoopDev& d,
+                     bool& active)
+{
+    std::memset(&in, 0, sizeof(in));
+    active = false;
+    // host code of this library is built with -ffp-contract=off: these sums
+    // round like the contract-off oracle
+    const double mn = g.m[0] * g.n[0] + g.m[1] * g.n[1] + g.m[2] * g.n[2];
+    int type = DISCO_MATTER_NONE;
+    if (!(std::fabs(mn) < 1e-6)) type = mn > 0. ? DISCO_MATTER_VACANCY : DISCO_MATTER_INTERSTITIAL;
+    if (!g.apply || type == DISCO_MATTER_NONE) return DISCO_OK;
+    if (g.shape < 0 || g.shape > DISCO_SHAPE_POLYGON || g.n_poly < 0 || g.n_poly > DISCO_MAX_POLY ||
+        !(g.spacing > 0.)) {
+        (void)l;
+        disco::set_last_error("bad slab loop: shape, polygon size or spacing out of range");
+        return DISCO_EINVAL;
+    }
+    in.type = type;
+    for (int i = 0; i < 3; ++i) in.b[i] = g.bmag * g.m[i];
+    in.height = std::fabs(in.b[0] * g.n[0] + in.b[1] * g.n[1] + in.b[2] * g.n[2]);
+    in.spacing = g.spacing;
+    const double ratio = in.height / g.spacing;
+    in.planes = (int)std::lround(ratio);
+    if (in.planes < 1 || std::fabs(ratio - in.planes) > 1e-6) {
+        disco::set_last_error("|b.n| is not a whole number of plane spacings");
+        return DISCO_EPLANES;
+    }
+    std::memset(&d, 0, sizeof(d));
+    d.L = g;
+    d.tLo = -std::floor(in.planes / 2.);
+    d.tHi = std::ceil(in.planes / 2.);
+    const double c = g.u[0] * g.v[0] + g.u[1] * g.v[1] + g.u[2] * g.v[2];
+    d.cuv = c;
+    d.det = 1.0 - c * c;
+    d.type = type;
+    active = true;
+    return DISCO_OK;
+}
+
+// Active loops in caller order.
 int prepare_loops(const disco_slab_loop* loops, int nloops, disco_slab_info* info,
                   std::vector<disco::SlabLoopDev>& act, std::vector<int>& act_index)
 {
     for (int l = 0; l < nloops; ++l) {
-        const disco_slab_loop& g = loops[l];
-        disco_slab_info& in = info[l];
-        std::memset(&in, 0, sizeof(in));
-        // host code of this library is built with -ffp-contract=off: these sums
-        // round like the contract-off oracle
-        const double mn = g.m[0] * g.n[0] + g.m[1] * g.n[1] + g.m[2] * g.n[2];
-        int type = DISCO_MATTER_NONE;
-        if (!(std::fabs(mn) < 1e-6)) type = mn > 0. ? DISCO_MATTER_VACANCY : DISCO_MATTER_INTERSTITIAL;
-        if (!g.apply || type == DISCO_MATTER_NONE) continue;
-        if (g.shape < 0 || g.shape > DISCO_SHAPE_POLYGON || g.n_poly < 0 || g.n_poly > DISCO_MAX_POLY ||
-            !(g.spacing > 0.)) {
-            return efail(DISCO_EINVAL, "bad slab loop " + std::to_string(l));
-        }
-        in.type = type;
-        for (int i = 0; i < 3; ++i) in.b[i] = g.bmag * g.m[i];
-        in.height = std::fabs(in.b[0] * g.n[0] + in.b[1] * g.n[1] + in.b[2] * g.n[2]);
-        in.spacing = g.spacing;
-        const double ratio = in.height / g.spacing;
-        in.planes = (int)std::lround(ratio);
-        if (in.planes < 1 || std::fabs(ratio - in.planes) > 1e-6) {
-            return efail(DISCO_EPLANES, "loop " + std::to_string(l) +
-                                        ": |b.n| is not a whole number of plane spacings");
-        }
-        if ((int)act.size() >= disco::kMaxSlabLoops) {
-            return efail(DISCO_ELIMIT, "more than 64 prismatic loops in one call");
-        }
         disco::SlabLoopDev d;
-        std::memset(&d, 0, sizeof(d));
-        d.L = g;
-        d.tLo = -std::floor(in.planes / 2.);
-        d.tHi = std::ceil(in.planes / 2.);
-        const double c = g.u[0] * g.v[0] + g.u[1] * g.v[1] + g.u[2] * g.v[2];
-        d.cuv = c;
-        d.det = 1.0 - c * c;
-        d.type = type;
+        bool active = false;
+        const int st = slab_loop_record(loops[l], l, info[l], d, active);
+        if (st) return st;
+        if (!active) continue;
+        if ((int)act.size() >= disco::kMaxSlabLoops) {
+            disco::set_last_error("more than 64 prismatic loops in one call");
+            return DISCO_ELIMIT;
+        }
         act.push_back(d);
         act_index.push_back(l);
     }
@@ -620,6 +636,171 @@ int disco_b200_finalize(const double* x, const double* y, const double* z,
     for (int k = 0; k < (want_u ? 6 : 3) && e == cudaSuccess; ++k)
         e = cudaMemcpy(dst[k], o + k * tot, (size_t)tot * sizeof(double), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cfail(e, "finalize");
+    return DISCO_OK;
+}
+
+} // extern "C"
+
+// ---- matter step without allocation ---------------------------------------------------
+//
+// Callers that own all device memory themselves (a framework with its own
+// memory pool, a code that may not synchronise the device the way cudaFree
+// does, a process with a fixed memory budget) cannot let the library call
+// cudaMalloc.  disco_b200_prismatic_noalloc takes device inputs and outputs
+// from the caller and keeps its scratch (active loop table, per-tile counts
+// and offsets, totals) in the file-scope array below: 1.25 MiB that every GPU
+// loading this library holds until the process exits.
+
+namespace {
+
+constexpr int64_t kNoAllocMaxAtoms = int64_t(1) << 22;                  // 4 194 304 atoms
+constexpr int64_t kNoAllocMaxTiles = kNoAllocMaxAtoms / disco::kSlabTile;
+constexpr size_t kNoAllocLoopBytes = disco::kMaxSlabLoops * sizeof(disco::SlabLoopDev);
+constexpr size_t kNoAllocTotalsBytes = (2 * (disco::kMaxSlabLoops + 1) + 1) * sizeof(int64_t);
+constexpr size_t kNoAllocTileBytes = kNoAllocMaxTiles * (disco::kMaxSlabLoops + 1) * sizeof(int32_t);
+constexpr size_t kNoAllocScratchBytes = 1280 * 1024;
+static_assert(((kNoAllocLoopBytes + 255) & ~size_t(255)) + ((kNoAllocTotalsBytes + 255) & ~size_t(255)) +
+                  2 * kNoAllocTileBytes <= kNoAllocScratchBytes,
+              "no-alloc scratch layout");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// array's name is a host-side stand-in, not a device address: the address is
+// looked up once per device with that device current and cached.
+int noalloc_scratch(unsigned char** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cfail(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices) return efail(DISCO_ELIMIT, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) return cfail(e, "cudaGetSymbolAddress of the scratch array");
+        g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return DISCO_OK;
+}
+
+size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
+
+} // namespace
+
+extern "C" {
+
+int disco_b200_prismatic_noalloc(const double* x, const double* y, const double* z, int64_t n,
+                                 const disco_slab_loop* loops, int32_t nloops, const double box[3],
+                                 double* x_out, double* y_out, double* z_out, int32_t* new_index,
+                                 disco_slab_info* info,
+                                 int32_t* slab_atoms, int8_t* slab_side, int64_t slab_capacity,
+                                 disco_copy* copies, int64_t copy_capacity,
+                                 int64_t counts[3], void* stream)
+{
+    using namespace disco;
+    if (n < 0 || nloops < 0 || !box || !counts || (nloops > 0 && (!loops || !info)) ||
+        (n > 0 && (!x || !y || !z || !x_out || !y_out || !z_out || !new_index)) ||
+        slab_capacity < 0 || copy_capacity < 0 || (slab_capacity > 0 && (!slab_atoms || !slab_side)) ||
+        (copy_capacity > 0 && !copies))
+        return efail(DISCO_EINVAL, "null or negative argument");
+    if (!(box[0] > 0.) || !(box[1] > 0.) || !(box[2] > 0.)) return efail(DISCO_EINVAL, "box lengths must be positive");
+    if (n > kNoAllocMaxAtoms)
+        return efail(DISCO_ELIMIT, "disco_b200_prismatic_noalloc takes at most 4194304 atoms (its scratch array is fixed)");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* base = nullptr;
+    int st = noalloc_scratch(&base);
+    if (st) return st;
+    SlabLoopDev* d_loops = reinterpret_cast<SlabLoopDev*>(base);
+    int64_t* d_tot = reinterpret_cast<int64_t*>(base + align256(kNoAllocLoopBytes));
+    int32_t* d_cnt = reinterpret_cast<int32_t*>(base + align256(kNoAllocLoopBytes) + align256(kNoAllocTotalsBytes));
+    int32_t* d_off = d_cnt + kNoAllocMaxTiles * (kMaxSlabLoops + 1);
+
+    // active loops, one record at a time from the stack (no host allocation)
+    int nl = 0;
+    int act_index[kMaxSlabLoops];
+    cudaError_t e = cudaSuccess;
+    for (int l = 0; l < nloops; ++l) {
+        SlabLoopDev d;
+        bool active = false;
+        st = slab_loop_record(loops[l], l, info[l], d, active);
+        if (st) return st;
+        if (!active) continue;
+        if (nl >= kMaxSlabLoops) return efail(DISCO_ELIMIT, "more than 64 prismatic loops in one call");
+        e = cudaMemcpyAsync(d_loops + nl, &d, sizeof(d), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cfail(e, "loop table upload");
+        act_index[nl++] = l;
+    }
+    const int C = nl + 1;
+    const int64_t ntiles = (n + kSlabTile - 1) / kSlabTile;
+    // the array keeps the previous call's contents: the totals must start at zero
+    e = cudaMemsetAsync(d_tot, 0, kNoAllocTotalsBytes, s);
+    if (e != cudaSuccess) return cfail(e, "totals reset");
+
+    SlabArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.x = x; a.y = y; a.z = z;
+    a.n = n;
+    a.loops = d_loops;
+    a.nl = nl;
+    a.Lx = box[0]; a.Ly = box[1]; a.Lz = box[2];
+    a.tile_counts = d_cnt;
+    a.tile_offsets = d_off;
+    a.totals = d_tot;
+    a.xo = x_out; a.yo = y_out; a.zo = z_out;
+    a.new_index = new_index;
+    a.slab_atoms = slab_atoms;
+    a.slab_side = slab_side;
+    const size_t smem = (size_t)nl * sizeof(SlabLoopDev);
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(slab_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(slab_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cfail(e, "prismatic smem");
+    }
+    if (ntiles > 0) slab_count_kernel<<<(unsigned)ntiles, kSlabThreads, smem, s>>>(a);
+    slab_scan_kernel<<<1, 1024, 0, s>>>(a, ntiles);
+    int64_t tot[2 * (kMaxSlabLoops + 1) + 1];
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(tot, d_tot, (size_t)(2 * C) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cfail(e, "prismatic count/scan");
+    int64_t slab_total = 0, inter_total = 0;
+    for (int q = 0; q < nl; ++q) {
+        slab_total += tot[1 + q];
+        // copies can only come from interstitial slabs
+        disco_slab_info& in = info[act_index[q]];
+        if (in.type == DISCO_MATTER_INTERSTITIAL) inter_total += tot[1 + q];
+        in.offset = tot[C + q];
+        in.count = tot[1 + q];
+    }
+    {
+        int64_t next = slab_total;
+        for (int l = nloops - 1; l >= 0; --l) {
+            if (info[l].type == DISCO_MATTER_NONE) info[l].offset = next;
+            else next = info[l].offset;
+        }
+    }
+    counts[0] = tot[0];
+    counts[1] = slab_total;
+    counts[2] = inter_total;         // upper bound until the copies pass has run
+    if (slab_total > slab_capacity)
+        return efail(DISCO_ELIMIT, "slab capacity too small (counts[1] holds the size needed)");
+    if (ntiles > 0) slab_scatter_kernel<<<(unsigned)ntiles, kSlabThreads, smem, s>>>(a);
+    slab_copies_kernel<<<1, 1024, 0, s>>>(a, copies, copy_capacity);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&tot[2 * C - 1], d_tot + (2 * C - 1), sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cfail(e, "prismatic scatter");
+    counts[2] = tot[2 * C - 1];
+    if (counts[2] > copy_capacity)
+        return efail(DISCO_ELIMIT, "copy capacity too small (counts[2] holds the size needed)");
     return DISCO_OK;
 }
 

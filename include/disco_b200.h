@@ -229,6 +229,32 @@ int disco_b200_prismatic(const double *x, const double *y, const double *z, int6
                          disco_copy *copies, int64_t copy_capacity,
                          int64_t counts[3]);
 
+/* The matter step above for callers that cannot let this library allocate
+ * device memory (their own allocator owns the GPU, or cudaMalloc/cudaFree and
+ * the device synchronisation they imply are not allowed where they call).
+ * No counterpart in the reference.  Inputs x, y, z and every output array
+ * except info and counts are DEVICE pointers the caller allocated; loops,
+ * box, info and counts are host memory.  Work is queued on `stream` (a
+ * cudaStream_t; NULL = legacy default stream) and the call waits for it twice
+ * to read the totals.  Scratch lives in a fixed 1.25 MiB device array inside
+ * the library (held by every GPU that loads it until the process exits):
+ * at most 4 194 304 atoms and 64 prismatic loops per call, DISCO_ELIMIT
+ * beyond.  The first call on a device looks up that array's device address
+ * (once per device), so make it before any stream capture.  All calls share
+ * the array: calls whose work overlaps on the GPU (other streams, other host
+ * threads on the same device) race and must be serialised by the caller.
+ * Capacities: slab_capacity as for disco_b200_prismatic; copies beyond
+ * copy_capacity are not written and the call returns DISCO_ELIMIT with
+ * counts[2] = copies needed.  The device outputs match disco_b200_prismatic's
+ * bit for bit. */
+int disco_b200_prismatic_noalloc(const double *x, const double *y, const double *z, int64_t n,
+                                 const disco_slab_loop *loops, int32_t nloops, const double box[3],
+                                 double *x_out, double *y_out, double *z_out, int32_t *new_index,
+                                 disco_slab_info *info,
+                                 int32_t *slab_atoms, int8_t *slab_side, int64_t slab_capacity,
+                                 disco_copy *copies, int64_t copy_capacity,
+                                 int64_t counts[3], void *stream);
+
 /* Code/main.cpp:733-743 and 797-818 fused: appends the copies (position of the
  * source, displacement u(source) + shift) after the n atoms, then writes the
  * wrapped final positions r = x + u, folded once into [-L/2, L/2] and shifted

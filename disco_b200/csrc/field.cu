@@ -33,7 +33,7 @@
 namespace disco {
 
 int build_table(const disco_loop* loops, int nloops, int kind, int precision, double nu,
-                HostTable& T, std::string& err)
+                HostTable& T, std::string& err, uint32_t stage_cap)
 {
     T = HostTable();
     T.kind = kind;
@@ -57,35 +57,13 @@ int build_table(const disco_loop* loops, int nloops, int kind, int precision, do
             for (int k0 = 0; k0 < nv; k0 += kMaxLinePiece) {
                 const int k1e = std::min(nv, k0 + kMaxLinePiece);
                 LinePiece p;
-                std::memset(&p, 0, sizeof(p));
-                const int a = (k0 + nv - 1) % nv;
-                p.ax = lp.vx[a]; p.ay = lp.vy[a]; p.az = lp.vz[a];
-                p.cx = lp.cx; p.cy = lp.cy; p.cz = lp.cz;
-                p.bx = bx; p.by = by; p.bz = bz;
-                p.nseg = k1e - k0;
                 std::vector<LineSeg> recs;
-                for (int k = k0; k < k1e; ++k) {
-                    const int km = (k + nv - 1) % nv;
-                    LineSeg s;
-                    std::memset(&s, 0, sizeof(s));
-                    s.vx = lp.vx[k]; s.vy = lp.vy[k]; s.vz = lp.vz[k];
-                    const double tx = lp.vx[k] - lp.vx[km], ty = lp.vy[k] - lp.vy[km],
-                                 tz = lp.vz[k] - lp.vz[km];
-                    const double L = std::sqrt(tx * tx + ty * ty + tz * tz);
-                    if (L > 0.0) {
-                        s.len = L;
-                        s.tx = tx / L; s.ty = ty / L; s.tz = tz / L;
-                        s.wx = by * s.tz - bz * s.ty;
-                        s.wy = bz * s.tx - bx * s.tz;
-                        s.wz = bx * s.ty - by * s.tx;
-                    }
-                    recs.push_back(s);
-                }
+                make_line_piece(lp, k0, k1e, bx, by, bz, p, recs);
                 L.pieces.push_back(p);
                 L.recs.push_back(std::move(recs));
             }
         }
-        pack_chunks(L, T);
+        pack_chunks(L, T, stage_cap);
     } else {
         PieceList<LooponPiece, LooponRec> L;
         for (int l = 0; l < nloops; ++l) {
@@ -125,7 +103,7 @@ int build_table(const disco_loop* loops, int nloops, int kind, int precision, do
                 L.recs.push_back(std::move(recs));
             }
         }
-        pack_chunks(L, T);
+        pack_chunks(L, T, stage_cap);
     }
     return DISCO_OK;
 }

@@ -27,6 +27,8 @@ struct alignas(16) LinePiece {
     double ax, ay, az;   // vertex before the piece's first segment
     double cx, cy, cz;   // fan apex (loop centre)
     double bx, by, bz;   // Burgers vector (phys.b * m)
+    double rho;          // largest |vertex - apex| over the piece's vertices
+    double lmax;         // longest segment of the piece
     int32_t nseg;        // segments of this piece
     int32_t rec;         // first segment record, index into the chunk's records
 };
@@ -36,7 +38,7 @@ struct alignas(16) LineSeg {
     double tx, ty, tz;   // unit tangent (B - A) / |B - A| (0 for a null segment)
     double wx, wy, wz;   // w = b x t
 };
-static_assert(sizeof(LinePiece) == 80 && sizeof(LineSeg) == 80, "line table layout");
+static_assert(sizeof(LinePiece) == 96 && sizeof(LineSeg) == 80, "line table layout");
 
 // ---- FP64 loopon method (Code/kroupa.hpp:52-73) ---------------------------------
 struct alignas(16) LooponPiece {
@@ -138,8 +140,12 @@ struct HostTable {
 
 // Builds the table of the loops of one kind (kLineKind: loops with line != 0,
 // kLooponKind: the others); returns DISCO_OK or an error code.
+// stage_cap: 0 = automatic chunking, > 0 = streamed chunks of at most stage_cap
+// bytes (which must hold the largest piece: 20.6 KB line, 46.2 KB loopon).
 int build_table(const disco_loop* loops, int nloops, int kind, int precision, double nu,
-                HostTable& out, std::string& err);
+                HostTable& out, std::string& err, uint32_t stage_cap = 0);
+int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, HostTable& out,
+                     std::string& err, uint32_t stage_cap = 0);
 
 // Picks the image split factor and grid and launches the kernel on `stream`.
 int launch_field(const FieldArgs& args, int kind, bool fp32, int sm_count, int threads_hint,

@@ -32,29 +32,50 @@ __device__ __forceinline__ void image_shift(int img, int images, double Lx, doub
     sz = Lz * kk;
 }
 
-// Field at P (an atom moved by minus an image shift) of one line piece.
-// Follows Code/barnett.hpp:55-106 term by term (see the file header for the
-// reformulations); adds b Omega/(4 pi) + the line terms to (ux, uy, uz).
-__device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineSeg* seg,
-                                                double Px, double Py, double Pz, double cJ, double cK,
-                                                double& ux, double& uy, double& uz)
+// 1/y for a positive normal y: the hardware approximation (rcp.approx.ftz.f64)
+// refined by one cubic Newton-Raphson step r = r0 (1 + e + e^2), e = 1 - y r0,
+// which takes its ~2^-22 relative error below the double rounding.
+__device__ __forceinline__ double rcp_nr(double y)
 {
-    // unit vector from P to the fan apex
-    const double r1x = pc.cx - Px, r1y = pc.cy - Py, r1z = pc.cz - Pz;
-    const double il1 = rsqrt(r1x * r1x + r1y * r1y + r1z * r1z);
-    const double ex = r1x * il1, ey = r1y * il1, ez = r1z * il1;
+    double r0;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r0) : "d"(y));
+    const double e = fma(-y, r0, 1.0);
+    return fma(r0, fma(e, e, e), r0);
+}
 
-    // vertex A (start of the current segment) relative to P
-    double ax = pc.ax - Px, ay = pc.ay - Py, az = pc.az - Pz;
-    double ila = rsqrt(ax * ax + ay * ay + az * az);
-    double la = (ax * ax + ay * ay + az * az) * ila;
+// Largest t = L/(RA+RB) for which the 8-term series of 2 atanh(t) is exact to
+// the double rounding: its remainder relative to the sum is below t^16/17.
+constexpr double kSeriesTau = 0.11;
+
+// J0 = ln((S+L)/(S-L)) = 2 atanh(t), t = L/S:  2 t (1 + t^2/3 + ... + t^14/15).
+__device__ __forceinline__ double j0_series(double t)
+{
+    const double t2 = t * t;
+    double p = 1.0 / 15.0;
+    p = fma(p, t2, 1.0 / 13.0);
+    p = fma(p, t2, 1.0 / 11.0);
+    p = fma(p, t2, 1.0 / 9.0);
+    p = fma(p, t2, 1.0 / 7.0);
+    p = fma(p, t2, 1.0 / 5.0);
+    p = fma(p, t2, 1.0 / 3.0);
+    p = fma(p, t2, 1.0);
+    return 2.0 * t * p;
+}
+
+// The segment loop of one line piece.  FAR: every segment of the piece is far
+// enough from P (for every lane of the warp) that J0 comes from the series.
+template <bool FAR>
+__device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, double Px, double Py, double Pz,
+                                              double ex, double ey, double ez, double ax, double ay, double az,
+                                              double cJ, double cK, double& zr, double& zi,
+                                              double& lx, double& ly, double& lz)
+{
+    const double la2 = ax * ax + ay * ay + az * az;
+    double ila = rsqrt(la2);
+    double la = la2 * ila;
     double hax = ax * ila, hay = ay * ila, haz = az * ila;
     double ca = ex * hax + ey * hay + ez * haz;                 // e . a-hat
     double qx = ey * haz - ez * hay, qy = ez * hax - ex * haz, qz = ex * hay - ey * hax;   // e x a-hat
-
-    double zr = 1.0, zi = 0.0;                                   // running product
-    double lx = 0.0, ly = 0.0, lz = 0.0;
-    const int nseg = pc.nseg;
     for (int k = 0; k < nseg; ++k) {
         const LineSeg s = seg[k];
         const double bx = s.vx - Px, by = s.vy - Py, bz = s.vz - Pz;
@@ -79,9 +100,11 @@ __device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineS
         const double d2 = dx * dx + dy * dy + dz * dz;
         const double dw = dx * s.wx + dy * s.wy + dz * s.wz;
         const double sum = la + lb;
-        const double J0 = log((sum + s.len) / (sum - s.len));
+        double J0;
+        if (FAR) J0 = j0_series(s.len * rcp_nr(sum));
+        else     J0 = log((sum + s.len) * rcp_nr(sum - s.len));
         const double g = sB * ilb - sA * ila;                   // d^2 K0
-        const double q = d2 > 0.0 ? dw / d2 : 0.0;
+        const double q = d2 > 0.0 ? dw * rcp_nr(d2) : 0.0;
         const double K1 = ila - ilb;
         const double al = cK * q * g, be = cK * dw * K1, ga = cJ * J0;
         lx += ga * s.wx - al * dx - be * s.tx;
@@ -94,10 +117,34 @@ __device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineS
         ca = cb;
         qx = ey * hbz - ez * hby; qy = ez * hbx - ex * hbz; qz = ex * hby - ey * hbx;
         if ((k & 63) == 63) {                                   // keep |z| near 1
-            const double sc = 1.0 / (fabs(zr) + fabs(zi));
+            const double sc = rcp_nr(fabs(zr) + fabs(zi));
             zr *= sc; zi *= sc;
         }
     }
+}
+
+// Field at P (an atom moved by minus an image shift) of one line piece.
+// Follows Code/barnett.hpp:55-106 term by term (see field.cu's header for the
+// reformulations); adds b Omega/(4 pi) + the line terms to (ux, uy, uz).
+// For every segment, RA + RB >= 2 (l1 - rho) with l1 = |apex - P| and rho the
+// piece's largest vertex radius, so t = L/(RA+RB) <= lmax / (2 (l1 - rho)).
+__device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineSeg* seg,
+                                                double Px, double Py, double Pz, double cJ, double cK,
+                                                double& ux, double& uy, double& uz)
+{
+    // unit vector from P to the fan apex
+    const double r1x = pc.cx - Px, r1y = pc.cy - Py, r1z = pc.cz - Pz;
+    const double l1sq = r1x * r1x + r1y * r1y + r1z * r1z;
+    const double il1 = rsqrt(l1sq);
+    const double ex = r1x * il1, ey = r1y * il1, ez = r1z * il1;
+    const double gap = l1sq * il1 - pc.rho;
+    const bool far_lane = gap > 0.0 && pc.lmax <= 2.0 * kSeriesTau * gap;
+    const bool far = __all_sync(__activemask(), far_lane);
+
+    double zr = 1.0, zi = 0.0, lx = 0.0, ly = 0.0, lz = 0.0;
+    const double ax = pc.ax - Px, ay = pc.ay - Py, az = pc.az - Pz;
+    if (far) line_segments<true>(seg, pc.nseg, Px, Py, Pz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz);
+    else     line_segments<false>(seg, pc.nseg, Px, Py, Pz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz);
     const double f = atan2(zi, zr) * (1.0 / 6.283185307179586476925286766559);   // Omega / (4 pi)
     ux += pc.bx * f + lx;
     uy += pc.by * f + ly;
@@ -282,19 +329,66 @@ __global__ void __launch_bounds__(kThreads, Policy::kMinBlocks) field_kernel(con
 
 // ---- host: tables -----------------------------------------------------------------------
 
+
+// One FP64 line piece: segments k0..k1e-1 of loop lp (segment k runs from
+// vertex k-1 to vertex k; Code/barnett.hpp:62-65), with everything that does
+// not depend on the atom precomputed.  rec is left to the chunk packer.
+inline void make_line_piece(const disco_loop& lp, int k0, int k1e, double bx, double by, double bz,
+                            LinePiece& p, std::vector<LineSeg>& recs)
+{
+    const int nv = lp.n_vertices;
+    std::memset(&p, 0, sizeof(p));
+    const int a = (k0 + nv - 1) % nv;
+    p.ax = lp.vx[a]; p.ay = lp.vy[a]; p.az = lp.vz[a];
+    p.cx = lp.cx; p.cy = lp.cy; p.cz = lp.cz;
+    p.bx = bx; p.by = by; p.bz = bz;
+    p.nseg = k1e - k0;
+    auto radius = [&](int k) {
+        const double dx = lp.vx[k] - lp.cx, dy = lp.vy[k] - lp.cy, dz = lp.vz[k] - lp.cz;
+        return std::sqrt(dx * dx + dy * dy + dz * dz);
+    };
+    p.rho = radius(a);
+    recs.clear();
+    for (int k = k0; k < k1e; ++k) {
+        const int km = (k + nv - 1) % nv;
+        LineSeg s;
+        std::memset(&s, 0, sizeof(s));
+        s.vx = lp.vx[k]; s.vy = lp.vy[k]; s.vz = lp.vz[k];
+        const double tx = lp.vx[k] - lp.vx[km], ty = lp.vy[k] - lp.vy[km], tz = lp.vz[k] - lp.vz[km];
+        const double L = std::sqrt(tx * tx + ty * ty + tz * tz);
+        if (L > 0.0) {
+            s.len = L;
+            s.tx = tx / L; s.ty = ty / L; s.tz = tz / L;
+            s.wx = by * s.tz - bz * s.ty;
+            s.wy = bz * s.tx - bx * s.tz;
+            s.wz = bx * s.ty - by * s.tx;
+        }
+        p.rho = std::max(p.rho, radius(k));
+        p.lmax = std::max(p.lmax, L);
+        recs.push_back(s);
+    }
+    // a little slack so that rounding in the kernel's bound never matters
+    p.rho *= 1.0 + 1e-12;
+    p.lmax *= 1.0 + 1e-12;
+}
+
 template <class Piece, class Rec>
 struct PieceList {
     std::vector<Piece> pieces;
     std::vector<std::vector<Rec>> recs;
 };
 
+// Packs the pieces into chunks.  stage_cap == 0: one resident chunk when the
+// table fits in kResidentMax, else stages of kStageMax; stage_cap > 0: stages
+// of at most stage_cap bytes (never resident, as the batched kernel needs).
 template <class Piece, class Rec>
-void pack_chunks(PieceList<Piece, Rec>& L, HostTable& T)
+void pack_chunks(PieceList<Piece, Rec>& L, HostTable& T, uint32_t stage_cap = 0)
 {
     size_t total = 0;
     for (size_t i = 0; i < L.pieces.size(); ++i) total += sizeof(Piece) + L.recs[i].size() * sizeof(Rec);
-    const uint32_t cap = total <= kResidentMax ? kResidentMax : kStageMax;
-    T.resident = total <= kResidentMax;
+    const bool resident = stage_cap == 0 && total <= kResidentMax;
+    const uint32_t cap = resident ? kResidentMax : (stage_cap ? stage_cap : kStageMax);
+    T.resident = resident;
     T.bytes.clear();
     T.chunks.clear();
     size_t i = 0;
@@ -330,7 +424,7 @@ void pack_chunks(PieceList<Piece, Rec>& L, HostTable& T)
         max_bytes = std::max(max_bytes, c.bytes);
         i = j;
     }
-    if (T.chunks.size() <= 1) T.resident = true;
+    if (T.chunks.size() <= 1 && stage_cap == 0) T.resident = true;
     T.stage_bytes = max_bytes;
 }
 

@@ -51,11 +51,13 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--config", default="fcc_random")
-    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
+    p.add_argument("--precision", default=None, choices=["fp64", "fp32c"],
+                   help="default: fp64, fp32c for the batch workload")
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--image-split", type=int, default=0)
+    p.add_argument("--samples", type=int, default=256, help="batch workload: number of samples")
     p.add_argument("--images", type=int, default=None,
                    help="override the workload's image range (profiling of small cases)")
     return p.parse_args()
@@ -362,10 +364,151 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """Config 4: 256 independent BCC samples in one persistent, graph-captured
+    launch (FP32 compensated by default), knobs from the autotuner."""
+    import torch
+    import torch.distributed as dist
+    from disco_b200 import autotune as A
+    from disco_b200 import backend as B
+    from disco_b200 import _capi as C
+    from disco_b200 import workloads as W
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    prec = C.DISCO_FP64 if args.precision == "fp64" else C.DISCO_FP32C
+    batch = W.batch(nsamples=args.samples)
+    tune = A.tune(batch, prec, log=(lambda m: print(m, file=sys.stderr)) if rank == 0 else None)
+    n = sum(w.n for w in batch)
+    evals = sum(w.n * w.evals_per_atom() for w in batch)
+    pos = [torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda") for w in batch]
+    u = [torch.zeros_like(p) for p in pos]
+    ptrs = [(p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr(), q[0].data_ptr(), q[1].data_ptr(),
+             q[2].data_ptr()) for p, q in zip(pos, u)]
+    plan = B.BatchPlan(batch, ptrs, precision=prec, image_split=tune["image_split"],
+                       stage_kb=tune["stage_kb"])
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        plan.execute(stream.cuda_stream)
+    plan.sync(stream.cuda_stream)
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.execute(stream.cuda_stream)
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    plan.sync(stream.cuda_stream)
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    per = elapsed / args.steps
+    # parity: a fresh sum on a few samples against the oracle
+    for q in u:
+        q.zero_()
+    plan.execute(stream.cuda_stream)
+    plan.sync(stream.cuda_stream)
+    parity = None
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        import oracle as O
+        rng = np.random.default_rng(7)
+        pick = rng.choice(len(batch), size=min(4, len(batch)), replace=False)
+        worst, t_cpu, ev_cpu, at_cpu = 0.0, 0.0, 0.0, 0
+        threads = os.cpu_count() or 1
+        for i in pick:
+            w = batch[i]
+            k = min(w.n, max(8, int(args.cpu_seconds * 2e8 / max(1.0, w.evals_per_atom()) / len(pick))))
+            idx = np.sort(rng.choice(w.n, size=k, replace=False))
+            t0 = time.perf_counter()
+            ref = O.displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box, images=w.images, nu=w.nu,
+                             threads=threads)
+            t_cpu += time.perf_counter() - t0
+            ev_cpu += k * w.evals_per_atom()
+            at_cpu += k
+            g = u[i].cpu().numpy()[:, idx]
+            worst = max(worst, float(np.abs(g - np.stack(ref)).max()))
+        parity = {"max_abs_du": worst, "atoms": at_cpu, "against": "oracle (FP64)"}
+        cpu = {"value": ev_cpu / t_cpu * n / evals, "unit": "atoms/s", "cores": threads, "kind": "port",
+               "sample": f"{at_cpu} random atoms of {len(pick)} samples, all their loops and images, "
+                         f"{t_cpu:.1f} s; rate converted to the whole batch's atoms via its "
+                         "evaluations per atom"}
+    # e2e: the public batched call on pinned host memory
+    e2e = None
+    if args.e2e_steps != 0:
+        hp = [torch.empty((6, w.n), dtype=torch.float64, pin_memory=True) for w in batch]
+        for w, h in zip(batch, hp):
+            hv = h.numpy()
+            hv[0], hv[1], hv[2] = w.x, w.y, w.z
+            hv[3:] = 0.0
+        arr, keep = B.sample_array(batch, us=[h.numpy()[3:] for h in hp])
+        for i, h in enumerate(hp):
+            hv = h.numpy()
+            arr[i].atoms = C.DiscoAtoms(*(hv[k].ctypes.data for k in range(6)), batch[i].n)
+        o = B.options(prec, 1, batch[0].nu, tune["image_split"])
+        o.stage_kb = tune["stage_kb"]
+        tm = C.DiscoTiming(0.0, 0.0, 0.0, None)
+        barrier()
+        t0 = time.perf_counter()
+        C.check(C.cuda_lib().disco_b200_batch(arr, len(batch), ctypes_byref(o), ctypes_byref(tm)))
+        barrier()
+        e2e_t = time.perf_counter() - t0
+        e2e = {"value": n * world / e2e_t, "unit": "atoms/s", "h2d_bytes_per_step": 48 * n,
+               "d2h_bytes_per_step": 24 * n, "steps": 1}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": n * world / per, "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == C.DISCO_FP64 else "f32c", "data": "synthetic",
+            "config": {"workload": "batch", "samples": len(batch), "atoms": n,
+                       "loops": sum(len(w.loops) for w in batch), "evals_per_step": evals,
+                       "images": "+-1..+-3 per sample", "nu": batch[0].nu,
+                       "precision": "fp64" if prec == C.DISCO_FP64 else "fp32c",
+                       "tuning": {"image_split": tune["image_split"], "stage_kb": tune["stage_kb"]},
+                       "graph": "one CUDA graph replay per step",
+                       "l2": f"inputs larger than L2 ({24 * n / 1e9:.2f} GB of positions)",
+                       "parallelism": f"replicas x{world}"},
+            "evals_per_s": evals * world / per,
+            "roofline": {"bound": "fp32" if prec != C.DISCO_FP64 else "fp64",
+                         "achieved": evals * W_LINE / per / 1e12, "peak": None, "unit": "TFLOP/s",
+                         "frac": None, "traffic": None},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": args.steps * (2 if prec == C.DISCO_FP32C else 1), "parity": parity,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def ctypes_byref(x):
+    import ctypes
+    return ctypes.byref(x)
+
+
 def main():
     args = parse()
+    if args.precision is None:
+        args.precision = "fp32c" if args.config == "batch" else "fp64"
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -47,7 +47,13 @@ class DiscoOptions(Structure):
     _fields_ = [("precision", c_int32), ("images", c_int32), ("nu", c_double),
                 ("chunk_pairs", c_double), ("atoms_per_thread", c_int32),
                 ("threads_per_block", c_int32), ("image_split", c_int32), ("verbose", c_int32),
-                ("near_plane", c_double), ("near_rim", c_double)]
+                ("near_plane", c_double), ("near_rim", c_double), ("stage_kb", c_int32),
+                ("reserved", c_int32)]
+
+
+class DiscoSample(Structure):
+    _fields_ = [("atoms", DiscoAtoms), ("loops", c_void_p), ("nloops", c_int32), ("images", c_int32),
+                ("box", D3)]
 
 
 class DiscoTiming(Structure):
@@ -133,6 +139,14 @@ def cuda_lib():
         _sig(lib, "disco_b200_plan_sync", c_int, [c_void_p, c_void_p])
         _sig(lib, "disco_b200_plan_stats", c_int, [c_void_p, POINTER(DiscoPlanStats)])
         _sig(lib, "disco_b200_plan_destroy", c_int, [c_void_p])
+        _sig(lib, "disco_b200_batch", c_int,
+             [POINTER(DiscoSample), c_int32, POINTER(DiscoOptions), POINTER(DiscoTiming)])
+        _sig(lib, "disco_b200_batch_plan_create", c_int,
+             [POINTER(DiscoSample), c_int32, POINTER(DiscoOptions), POINTER(c_void_p)])
+        _sig(lib, "disco_b200_batch_plan_execute", c_int, [c_void_p, c_void_p])
+        _sig(lib, "disco_b200_batch_plan_sync", c_int, [c_void_p, c_void_p])
+        _sig(lib, "disco_b200_batch_plan_stats", c_int, [c_void_p, POINTER(DiscoPlanStats)])
+        _sig(lib, "disco_b200_batch_plan_destroy", c_int, [c_void_p])
         _sig(lib, "disco_b200_prismatic", c_int,
              [c_void_p, c_void_p, c_void_p, c_int64, POINTER(DiscoSlabLoop), c_int32,
               POINTER(c_double), c_void_p, c_void_p, c_void_p, c_void_p, POINTER(DiscoSlabInfo),

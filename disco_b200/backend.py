@@ -233,3 +233,81 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def sample_array(workloads, us=None, device_ptrs=None):
+    """ctypes DiscoSample array for a batch (host arrays, or device pointers
+    given as [(x, y, z, ux, uy, uz), ...])."""
+    keep = []
+    arr = (C.DiscoSample * max(1, len(workloads)))()
+    for i, w in enumerate(workloads):
+        la, lk = loop_array(w.loops)
+        keep += [la, lk]
+        d = arr[i]
+        if device_ptrs is not None:
+            d.atoms = C.DiscoAtoms(*device_ptrs[i], w.n)
+        else:
+            u = us[i]
+            xs = [_f64(w.x), _f64(w.y), _f64(w.z)]
+            keep += xs
+            d.atoms = C.DiscoAtoms(xs[0].ctypes.data, xs[1].ctypes.data, xs[2].ctypes.data,
+                                   u[0].ctypes.data, u[1].ctypes.data, u[2].ctypes.data, w.n)
+        d.loops = ctypes.cast(la, ctypes.c_void_p)
+        d.nloops = len(w.loops)
+        d.images = w.images
+        d.box = C.D3(*w.box)
+    return arr, keep
+
+
+def batch_gpu(workloads, precision=C.DISCO_FP64, nu=None, image_split=0, stage_kb=0):
+    """The batched form on host arrays: returns [(ux, uy, uz)] per sample."""
+    lib = C.cuda_lib()
+    nu = workloads[0].nu if nu is None else nu
+    us = [[np.zeros(w.n), np.zeros(w.n), np.zeros(w.n)] for w in workloads]
+    arr, keep = sample_array(workloads, us)
+    o = options(precision, 1, nu, image_split)
+    o.stage_kb = stage_kb
+    tm = C.DiscoTiming(0.0, 0.0, 0.0, None)
+    C.check(lib.disco_b200_batch(arr, len(workloads), ctypes.byref(o), ctypes.byref(tm)), lib)
+    del keep
+    return us, tm.kernels
+
+
+class BatchPlan:
+    """Resident batched form: tables, unit queue and CUDA graph built once;
+    atoms are device arrays given as [(x, y, z, ux, uy, uz) pointers]."""
+
+    def __init__(self, workloads, device_ptrs, *, precision=C.DISCO_FP64, nu=None, image_split=0,
+                 stage_kb=0):
+        self._lib = C.cuda_lib()
+        nu = workloads[0].nu if nu is None else nu
+        arr, keep = sample_array(workloads, device_ptrs=device_ptrs)
+        o = options(precision, 1, nu, image_split)
+        o.stage_kb = stage_kb
+        h = ctypes.c_void_p()
+        C.check(self._lib.disco_b200_batch_plan_create(arr, len(workloads), ctypes.byref(o),
+                                                       ctypes.byref(h)), self._lib)
+        self._h = h
+        del keep
+
+    def execute(self, stream=0):
+        C.check(self._lib.disco_b200_batch_plan_execute(self._h, ctypes.c_void_p(stream)), self._lib)
+
+    def sync(self, stream=0):
+        C.check(self._lib.disco_b200_batch_plan_sync(self._h, ctypes.c_void_p(stream)), self._lib)
+
+    def stats(self):
+        s = C.DiscoPlanStats()
+        C.check(self._lib.disco_b200_batch_plan_stats(self._h, ctypes.byref(s)), self._lib)
+        return {k: getattr(s, k) for k, _ in C.DiscoPlanStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.disco_b200_batch_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -16,8 +16,6 @@
 
 namespace disco {
 int choose_split(int64_t n, int nimg, int resident_ctas);
-int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, HostTable& T,
-                     std::string& err);
 int launch_field_fp32(const FieldArgs& a, int kind, int sm_count, int split_hint,
                       cudaStream_t stream, std::string& err);
 }
@@ -74,6 +72,8 @@ int check_options(const disco_options& o)
     if (!(o.nu > -1.0 && o.nu < 0.5)) return fail(DISCO_EINVAL, "nu must be in (-1, 0.5)");
     if (!(o.near_plane >= 0.0) || !(o.near_rim >= 0.0))
         return fail(DISCO_EINVAL, "near_plane and near_rim must be >= 0");
+    if (o.stage_kb != 0 && (o.stage_kb < 16 || o.stage_kb > 100))
+        return fail(DISCO_EINVAL, "stage_kb must be 0 or in 16..100");
     if (o.image_split != 0 && (o.image_split < 1 || o.image_split > 32 ||
                                (o.image_split & (o.image_split - 1))))
         return fail(DISCO_EINVAL, "image_split must be 0 or a power of two up to 32");
@@ -191,9 +191,10 @@ int disco_b200_plan_create(const disco_loop* loops, int32_t nloops, const double
     for (int k = 0; k < 2; ++k) {
         std::string err;
         const int kind = k == 0 ? disco::kLineKind : disco::kLooponKind;
+        const uint32_t cap = o.stage_kb > 0 ? (uint32_t)o.stage_kb * 1024u : 0u;
         st = o.precision == DISCO_FP32C
-                 ? disco::build_table_fp32(loops, nloops, kind, o.nu, p->tables[k], err)
-                 : disco::build_table(loops, nloops, kind, o.precision, o.nu, p->tables[k], err);
+                 ? disco::build_table_fp32(loops, nloops, kind, o.nu, p->tables[k], err, cap)
+                 : disco::build_table(loops, nloops, kind, o.precision, o.nu, p->tables[k], err, cap);
         if (st) { free_plan(p); return fail(st, err); }
         const disco::HostTable& T = p->tables[k];
         for (int l = 0; l < nloops; ++l) p->loop_evals[l] += T.loop_evals[l];

@@ -148,6 +148,51 @@ def bcc_prismatic(cells=60, a0=3.165, nu=0.28, images=1, seed=3, n_inter=8, n_va
                     (cells, cells, cells), slab_loops=slabs, geom=geom)
 
 
+_N110 = [(1, 1, 0), (1, -1, 0), (1, 0, 1), (1, 0, -1), (0, 1, 1), (0, 1, -1)]
+_N112 = [(1, 1, 2), (1, 1, -2), (1, -1, 2), (-1, 1, 2), (1, 2, 1), (1, 2, -1), (1, -2, 1), (-1, 2, 1),
+         (2, 1, 1), (2, 1, -1), (2, -1, 1), (-2, 1, 1)]
+_B111 = [(1, 1, 1), (1, 1, -1), (1, -1, 1), (-1, 1, 1)]
+
+
+def batch(nsamples=256, a0=2.855, edge=(20, 80), nloops=(1, 32), radius=(8.0, 40.0),
+          segments=(16, 128), images=(1, 3), nu=0.29, seed=4, da=1.0):
+    """Many independent BCC samples for the batched form: box edges uniform
+    integers in `edge` (cells, independent per axis), 1-32 glide loops each
+    (circles of `segments` chords or regular hexagons, radius in `radius`), on
+    random {110}<111> or {112}<111> systems with a random sign of b, centres
+    uniform, images +-U{images}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(nsamples):
+        nx, ny, nz = (int(v) for v in rng.integers(edge[0], edge[1] + 1, size=3))
+        L = (nx * a0, ny * a0, nz * a0)
+        x, y, z = G.lattice(G.BCC, nx, ny, nz, a0)
+        loops, geom = [], []
+        for _ in range(int(rng.integers(nloops[0], nloops[1] + 1))):
+            fam = _N110 if rng.random() < 0.5 else _N112
+            n = fam[rng.integers(len(fam))]
+            bs = [b for b in _B111 if b[0] * n[0] + b[1] * n[1] + b[2] * n[2] == 0]
+            m = bs[rng.integers(len(bs))]
+            if rng.random() < 0.5:
+                m = tuple(-t for t in m)
+            c = np.array([rng.uniform(-l / 2, l / 2) for l in L])
+            cs, _ = G.snap(c, n, a0, nx, ny, nz, G.BCC)
+            R = rng.uniform(*radius)
+            if rng.random() < 0.5:
+                k = int(rng.integers(segments[0], segments[1] + 1))
+                lp = G.Loop.circle(da, R, cs, m, n, a0)
+                P = lp.polyline(G.circle_eps_for_chords(R, k))
+            else:
+                lp = G.Loop.polygon(da, G.regular_polygon(6, R, m, n), 0.0, cs, m, n, a0)
+                P = lp.polyline(0.01)
+            geom.append(lp)
+            loops.append(lp.line_data(vertices=P))
+        im = int(rng.integers(images[0], images[1] + 1))
+        out.append(Workload(f"batch[{s}]", x, y, z, loops, L, im, nu, "line", G.BCC, a0, (nx, ny, nz),
+                            geom=geom))
+    return out
+
+
 # Full-size workloads by name (bench and tests select them by these names).
 FULL = {
     "quadrupole": quadrupole,

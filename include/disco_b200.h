@@ -109,6 +109,9 @@ typedef struct {
                                   near_rim A beyond the loop's largest vertex radius
                                   is evaluated in FP64; 0 = defaults (3 A, 3 A)   */
     double  near_rim;
+    int32_t stage_kb;          /* shared-memory stage of the streamed tables, KB;
+                                  0 = automatic (resident up to 110 KB, else 48)  */
+    int32_t reserved;
 } disco_options;
 
 /* Phase timings, seconds: Code/backend.hpp:36-39 (BackendTiming).
@@ -168,6 +171,38 @@ int disco_b200_plan_stats(const disco_plan *plan, disco_plan_stats *stats);
  * device since the last call (DISCO_ETIMEOUT if a bounded wait gave up). */
 int disco_b200_plan_sync(disco_plan *plan, void *stream);
 int disco_b200_plan_destroy(disco_plan *plan);
+
+/* ---- batched form: many independent samples in one persistent launch ------------ */
+
+/* One sample: its atoms (host pointers for disco_b200_batch, device pointers
+ * for disco_b200_batch_plan_create), its loops (host), box and image range.
+ * nu and the precision are the batch's (disco_options). */
+typedef struct {
+    disco_atoms atoms;
+    const disco_loop *loops;
+    int32_t nloops;
+    int32_t images;
+    double box[3];
+} disco_sample;
+
+typedef struct disco_batch_plan disco_batch_plan;
+
+/* Batched form of disco_b200_displace (SURVEY's disco_b200_batch): every sample's
+ * field is added into its own u.  All samples run in one persistent launch per
+ * loop kind over a queue of (sample, atom tile, table chunk) units, balanced
+ * across the CTAs by their exact cost; opt->image_split and opt->stage_kb are
+ * the tuning knobs (0 = automatic). */
+int disco_b200_batch(const disco_sample *samples, int32_t nsamples, const disco_options *opt,
+                     disco_timing *timing);
+
+/* Resident form: tables, unit queue and a CUDA graph of the launches are built
+ * once; execute replays the graph on `stream` (device atoms given at create). */
+int disco_b200_batch_plan_create(const disco_sample *samples, int32_t nsamples,
+                                 const disco_options *opt, disco_batch_plan **out);
+int disco_b200_batch_plan_execute(disco_batch_plan *plan, void *stream);
+int disco_b200_batch_plan_sync(disco_batch_plan *plan, void *stream);
+int disco_b200_batch_plan_stats(const disco_batch_plan *plan, disco_plan_stats *stats);
+int disco_b200_batch_plan_destroy(disco_batch_plan *plan);
 
 /* ---- prismatic loops: slab selection and stream compaction ------------------------ */
 

@@ -147,6 +147,19 @@ def cuda_lib():
         _sig(lib, "disco_b200_batch_plan_sync", c_int, [c_void_p, c_void_p])
         _sig(lib, "disco_b200_batch_plan_stats", c_int, [c_void_p, POINTER(DiscoPlanStats)])
         _sig(lib, "disco_b200_batch_plan_destroy", c_int, [c_void_p])
+        _sig(lib, "disco_b200_mlp_create", c_int, [ctypes.c_uint64, POINTER(c_void_p)])
+        _sig(lib, "disco_b200_mlp_destroy", c_int, [c_void_p])
+        _sig(lib, "disco_b200_mlp_param_count", c_int, [])
+        _sig(lib, "disco_b200_mlp_get_params", c_int, [c_void_p, c_void_p])
+        _sig(lib, "disco_b200_mlp_set_params", c_int, [c_void_p, c_void_p])
+        _sig(lib, "disco_b200_mlp_get_grads", c_int, [c_void_p, c_void_p])
+        _sig(lib, "disco_b200_mlp_forward", c_int, [c_void_p, c_void_p, c_int64, c_void_p, c_void_p])
+        _sig(lib, "disco_b200_mlp_grad", c_int,
+             [c_void_p, c_void_p, c_void_p, c_int64, POINTER(ctypes.c_float), c_void_p])
+        _sig(lib, "disco_b200_mlp_adam", c_int,
+             [c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+              c_void_p])
+        _sig(lib, "disco_b200_mlp_status", c_int, [c_void_p])
         _sig(lib, "disco_b200_prismatic", c_int,
              [c_void_p, c_void_p, c_void_p, c_int64, POINTER(DiscoSlabLoop), c_int32,
               POINTER(c_double), c_void_p, c_void_p, c_void_p, c_void_p, POINTER(DiscoSlabInfo),

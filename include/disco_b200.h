@@ -204,6 +204,32 @@ int disco_b200_batch_plan_sync(disco_batch_plan *plan, void *stream);
 int disco_b200_batch_plan_stats(const disco_batch_plan *plan, disco_plan_stats *stats);
 int disco_b200_batch_plan_destroy(disco_batch_plan *plan);
 
+/* ---- learned far-image surrogate: the network ---------------------------------------
+ * The reference has no learned path; this is the network of the learned form
+ * (14 -> 128 -> 128 -> 128 -> 3, SiLU, BF16 weights and activations on the
+ * tensor cores, FP32 accumulation), trained and evaluated by this library's
+ * own tcgen05 kernels.  Features are padded to 16 columns and outputs to 16
+ * (X: n x 16, Y: n x 16, T: n x 3, all FP32 row-major DEVICE arrays).
+ * Parameters: W1[128x16] b1[128] W2[128x128] b2 W3[128x128] b3 W4[16x128] b4[16]
+ * as one FP32 vector of disco_b200_mlp_param_count() values. */
+typedef struct disco_mlp disco_mlp;
+
+int disco_b200_mlp_create(uint64_t seed, disco_mlp **out);
+int disco_b200_mlp_destroy(disco_mlp *m);
+int disco_b200_mlp_param_count(void);
+int disco_b200_mlp_get_params(const disco_mlp *m, float *host);
+int disco_b200_mlp_set_params(disco_mlp *m, const float *host);
+int disco_b200_mlp_get_grads(const disco_mlp *m, float *host);
+int disco_b200_mlp_forward(disco_mlp *m, const float *X, int64_t n, float *Y, void *stream);
+/* forward + backward of the mean squared error over n rows; gradients
+ * accumulate in the model until disco_b200_mlp_adam applies and clears them */
+int disco_b200_mlp_grad(disco_mlp *m, const float *X, const float *T, int64_t n, float *loss,
+                        void *stream);
+int disco_b200_mlp_adam(disco_mlp *m, float lr, float beta1, float beta2, float eps,
+                        float weight_decay, void *stream);
+/* waits for the device and reports a bounded wait of an MLP kernel that gave up */
+int disco_b200_mlp_status(disco_mlp *m);
+
 /* ---- prismatic loops: slab selection and stream compaction ------------------------ */
 
 /* One loop of the matter step.  Geometry as in the reference's loop class

@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--samples", type=int, default=256, help="batch workload: number of samples")
     p.add_argument("--images", type=int, default=None,
                    help="override the workload's image range (profiling of small cases)")
+    p.add_argument("--retrain", action="store_true", help="learned: train the network even if cached")
+    p.add_argument("--epochs", type=int, default=32, help="learned: training epochs over 2^22 samples")
+    p.add_argument("--no-fp64", action="store_true", help="learned: skip the plain FP64 comparison run")
     return p.parse_args()
 
 
@@ -146,6 +149,33 @@ def fp64_peak_tflops(torch):
     del a, b
     torch.cuda.empty_cache()
     return 2.0 * n ** 3 / best / 1e12
+
+
+def fp32_peak_tflops(torch):
+    """Dense FP32 CUDA-core throughput, measured with an SGEMM without TF32
+    (best of 5): the denominator of the FP32 kernels' roofline."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 8192
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e9
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1) * 1e-3)
+        del a, b
+        torch.cuda.empty_cache()
+        return 2.0 * n ** 3 / best / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
 
 
 def traffic_from_profiles(kernel_key):
@@ -325,7 +355,7 @@ def run_ours(args):
            "h2d_bytes_per_step": 6 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n, "steps": e2e_steps}
 
     if rank == 0:
-        peak = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else None
+        peak = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else fp32_peak_tflops(torch)
         flops = evals_atom * n * flop_per_eval(w)
         achieved = flops / per_launch / 1e12
         key = f"{'line' if w.method == 'line' else 'loopon'}_{args.precision}_{args.config}"
@@ -333,8 +363,9 @@ def run_ours(args):
         roof = {"bound": "fp64" if prec == C.DISCO_FP64 else "fp32", "achieved": achieved,
                 "peak": peak, "unit": "TFLOP/s", "frac": (achieved / peak) if peak else None,
                 "traffic": traffic,
-                "peak_source": "measured here: torch DGEMM 8192^3 best of 5 (MEASURED_PEAKS.json has no "
-                               "FP64 figure)" if peak else None,
+                "peak_source": ("measured here: torch DGEMM 8192^3 best of 5" if prec == C.DISCO_FP64 else
+                                "measured here: torch SGEMM 8192^3 without TF32, best of 5") +
+                               " (MEASURED_PEAKS.json has no FP64 or FP32 CUDA-core figure)",
                 "flop_per_eval": flop_per_eval(w), "evals_per_launch": evals_atom * n}
         cpu = None
         parity = None
@@ -496,6 +527,155 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
+def run_learned(args):
+    """Learned form on the fcc_random geometry with images +-4 (729 images):
+    exact near images +-1 (27, FP32 compensated), the network's far shells
+    2 <= max|n| <= 4 (702 images), the exact FP64 far-shell sum re-checked on a
+    1 % stratified random atom subsample every step with per-loop fallback.
+    The plain FP64 path on the same workload (all 729 images exact) is timed
+    once and judges the learned result on every atom."""
+    import torch
+    from disco_b200 import backend as B
+    from disco_b200 import _capi as C
+    from disco_b200 import learned as Ln
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    w = build_workload("fcc_random", 4)
+    n = w.n
+    log = (lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None
+    path = os.environ.get("DISCO_B200_FAR_NET",
+                          os.path.join(ROOT, "disco_b200", "_lib", f"far_fcc_random_nu{w.nu:.2f}.npz"))
+    if args.retrain and os.path.exists(path) and rank == 0:
+        os.remove(path)
+    if world > 1:
+        dist.barrier()
+    m, norm, info = Ln.cached_or_train(path if rank == 0 else None, log=log, nloops=4096, atoms=1024, seed=5,
+                                       nu=w.nu, epochs=args.epochs)
+    stream = torch.cuda.current_stream()
+    pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
+    u = torch.zeros_like(pos)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for s in range(args.warmup):
+        Ln.learned_displace(m, norm, pos, u, w.loops, w.box, w.nu, seed=s)
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = []
+    e0.record(stream)
+    for s in range(args.steps):
+        reps.append(Ln.learned_displace(m, norm, pos, u, w.loops, w.box, w.nu, seed=100 + s))
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    per = elapsed / args.steps
+
+    # accuracy on every atom against the plain FP64 path (+-4, all images exact)
+    ul = torch.zeros_like(pos)
+    rep = Ln.learned_displace(m, norm, pos, ul, w.loops, w.box, w.nu, seed=777)
+    acc, fp64 = None, None
+    if not args.no_fp64:
+        ux = torch.zeros_like(pos)
+        plan = B.Plan(w.loops, w.box, precision=C.DISCO_FP64, images=4, nu=w.nu, max_atoms=n)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        plan.execute(pos, ux)
+        f1.record(stream)
+        plan.sync(stream.cuda_stream)
+        t64 = f0.elapsed_time(f1) * 1e-3
+        st64 = plan.stats()
+        plan.close()
+        un = torch.zeros_like(pos)
+        pn = B.Plan(w.loops, w.box, precision=C.DISCO_FP32C, images=1, nu=w.nu, max_atoms=n)
+        pn.execute(pos, un)
+        pn.sync(stream.cuda_stream)
+        pn.close()
+        d = ul - ux
+        acc = {"max_abs_du": float(d.abs().max()), "rms_du": float(d.pow(2).mean().sqrt()),
+               "truncated_max_abs_du": float((un - ux).abs().max()),
+               "against": "plain FP64 path, images +-4, every atom"}
+        fp64 = {"value": n / t64, "unit": "atoms/s", "ms_per_step": 1e3 * t64, "steps": 1,
+                "evals_per_s": st64["evals_per_atom"] * n / t64}
+        del ux, un
+    # e2e: host positions in, host displacements out, every step
+    hp = torch.empty((6, n), dtype=torch.float64, pin_memory=True)
+    hv = hp.numpy()
+    hv[0], hv[1], hv[2] = w.x, w.y, w.z
+    hv[3:] = 0.0
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else 2
+    dpos = torch.empty_like(pos)
+    du_ = torch.empty_like(pos)
+    barrier()
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        dpos.copy_(hp[:3], non_blocking=True)
+        du_.copy_(hp[3:], non_blocking=True)
+        Ln.learned_displace(m, norm, dpos, du_, w.loops, w.box, w.nu, seed=500 + s)
+        hp[3:].copy_(du_, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_t = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_t], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e = {"value": n * world * e2e_steps / e2e_t, "unit": "atoms/s", "h2d_bytes_per_step": 48 * n,
+           "d2h_bytes_per_step": 24 * n, "steps": e2e_steps}
+    if rank == 0:
+        segs = sum(len(lp.vx) for lp in w.loops)
+        near_evals = segs * 27 * n
+        t_near = statistics.median(r["t_near"] for r in reps)
+        peak = fp32_peak_tflops(torch)
+        achieved = near_evals * W_LINE / t_near / 1e12
+        cpu = None
+        if not args.no_cpu:
+            cpu, idx, ucpu = cpu_baseline(w, args.cpu_seconds, use_reference=False)
+            cpu.pop("seconds", None)
+        mean = lambda k: statistics.mean(r[k] for r in reps)
+        line = {
+            "metric": METRIC, "value": n * world / per, "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32c+bf16",
+            "data": "synthetic",
+            "config": {"workload": "fcc_random_learned", "atoms": n, "loops": len(w.loops), "segments": segs,
+                       "images": 729, "near_images": 27, "far_images": 702, "nu": w.nu,
+                       "near": "exact, FP32 compensated", "far": "MLP 14-128-128-128-3, BF16 tcgen05",
+                       "check": "exact FP64 far shells on 1% of the atoms per step, per-loop fallback above "
+                                "1e-3 A", "l2": f"inputs larger than L2 (positions {24 * n / 1e6:.0f} MB)",
+                       "parallelism": f"replicas x{world}"},
+            "learned": {"speedup_vs_fp64": (fp64["ms_per_step"] / (1e3 * per)) if fp64 else None,
+                        "accuracy": acc, "n_fallback": [r["n_fallback"] for r in reps],
+                        "check_max": max(r["check_max"] for r in reps),
+                        "worst_loop": max(r["worst_loop"] for r in reps),
+                        "phase_seconds": {k: mean(k) for k in ("t_check", "t_near", "t_far", "t_fallback")},
+                        "training": {k: v for k, v in info.items() if k != "loss"}},
+            "fp64_exact": fp64,
+            "roofline": {"bound": "fp32", "kernel": "near-shell FP32 line kernel", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured here: torch SGEMM 8192^3 without TF32, best of 5",
+                         "flop_per_eval": W_LINE, "evals_per_launch": near_evals},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": sum(r["launches"] for r in reps),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def ctypes_byref(x):
     import ctypes
     return ctypes.byref(x)
@@ -509,6 +689,8 @@ def main():
         run_reference(args)
     elif args.config == "batch":
         run_batch(args)
+    elif args.config == "learned":
+        run_learned(args)
     else:
         run_ours(args)
 

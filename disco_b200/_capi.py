@@ -48,12 +48,12 @@ class DiscoOptions(Structure):
                 ("chunk_pairs", c_double), ("atoms_per_thread", c_int32),
                 ("threads_per_block", c_int32), ("image_split", c_int32), ("verbose", c_int32),
                 ("near_plane", c_double), ("near_rim", c_double), ("stage_kb", c_int32),
-                ("reserved", c_int32)]
+                ("image_min", c_int32)]
 
 
 class DiscoSample(Structure):
     _fields_ = [("atoms", DiscoAtoms), ("loops", c_void_p), ("nloops", c_int32), ("images", c_int32),
-                ("box", D3)]
+                ("box", D3), ("image_min", c_int32), ("reserved", c_int32)]
 
 
 class DiscoTiming(Structure):
@@ -91,6 +91,24 @@ class DiscoGeomLoop(Structure):
                 ("half_m", c_double), ("half_p", c_double), ("r_corner", c_double),
                 ("da", c_double), ("dS", c_double),
                 ("pu", DP), ("pv", DP), ("qu", DP), ("qv", DP), ("nu", DP), ("nv", DP)]
+
+
+class DiscoFarNorm(Structure):
+    _fields_ = [("mu", ctypes.c_float * 16), ("inv_sd", ctypes.c_float * 16), ("out_scale", ctypes.c_float),
+                ("images", c_int32), ("image_min", c_int32), ("reserved", c_int32)]
+
+
+class DiscoLearnedOptions(Structure):
+    _fields_ = [("precision", c_int32), ("check_precision", c_int32), ("nu", c_double),
+                ("check_fraction", c_double), ("tol_loop", c_double), ("tol_total", c_double),
+                ("seed", ctypes.c_uint64)]
+
+
+class DiscoLearnedReport(Structure):
+    _fields_ = [("n_check", c_int64), ("n_fallback", c_int32), ("launches", c_int32),
+                ("check_max", c_double), ("check_rms", c_double), ("worst_loop", c_double),
+                ("t_check", c_double), ("t_near", c_double), ("t_far", c_double), ("t_fallback", c_double),
+                ("loop_err", c_void_p), ("fallback", c_void_p)]
 
 
 class DiscoError(RuntimeError):
@@ -160,6 +178,15 @@ def cuda_lib():
              [c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
               c_void_p])
         _sig(lib, "disco_b200_mlp_status", c_int, [c_void_p])
+        _sig(lib, "disco_b200_far_features", c_int,
+             [POINTER(DiscoAtoms), POINTER(DiscoLoop), c_int32, POINTER(c_double), POINTER(DiscoFarNorm),
+              c_void_p, c_void_p, c_void_p])
+        _sig(lib, "disco_b200_far_apply", c_int,
+             [c_void_p, POINTER(DiscoFarNorm), POINTER(DiscoAtoms), POINTER(DiscoLoop), c_int32,
+              POINTER(c_double), c_void_p, c_int32, c_void_p, c_void_p])
+        _sig(lib, "disco_b200_learned_displace", c_int,
+             [c_void_p, POINTER(DiscoFarNorm), POINTER(DiscoAtoms), POINTER(DiscoLoop), c_int32,
+              POINTER(c_double), POINTER(DiscoLearnedOptions), POINTER(DiscoLearnedReport), c_void_p])
         _sig(lib, "disco_b200_prismatic", c_int,
              [c_void_p, c_void_p, c_void_p, c_int64, POINTER(DiscoSlabLoop), c_int32,
               POINTER(c_double), c_void_p, c_void_p, c_void_p, c_void_p, POINTER(DiscoSlabInfo),

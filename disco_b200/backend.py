@@ -119,7 +119,7 @@ def loop_array(loops):
 
 
 def options(precision=C.DISCO_FP64, images=1, nu=0.35, image_split=0, verbose=0, near_plane=0.0,
-            near_rim=0.0):
+            near_rim=0.0, image_min=0):
     lib = C.cuda_lib()
     o = C.DiscoOptions()
     lib.disco_b200_options_default(ctypes.byref(o))
@@ -130,6 +130,7 @@ def options(precision=C.DISCO_FP64, images=1, nu=0.35, image_split=0, verbose=0,
     o.verbose = verbose
     o.near_plane = near_plane
     o.near_rim = near_rim
+    o.image_min = image_min
     return o
 
 
@@ -156,14 +157,14 @@ def gpu_line_fp64():
 
 
 def kroupa_gpu(atoms, loops, dx, dy, dz, opt=None, t=None, *, images=1, nu=0.35, image_split=0,
-               verbose=0, near_plane=0.0, near_rim=0.0):
+               verbose=0, near_plane=0.0, near_rim=0.0, image_min=0):
     """kroupaGPU (Code/backend.hpp:61-62): adds the field of every loop over its
     periodic images into atoms.ux/uy/uz.  images and nu default to the
     reference's fixed values (+-1, 0.35).  Raises DiscoError on failure."""
     opt = opt or GpuOptions()
     lib = C.cuda_lib()
     o = options(C.DISCO_FP32C if opt.fp32 else C.DISCO_FP64, images, nu, image_split, verbose,
-                near_plane, near_rim)
+                near_plane, near_rim, image_min)
     o.chunk_pairs = opt.chunkPairs
     for name in ("x", "y", "z", "ux", "uy", "uz"):
         a = getattr(atoms, name)
@@ -189,9 +190,9 @@ class Plan:
     field into device arrays (torch tensors or raw device pointers)."""
 
     def __init__(self, loops, box, *, precision=C.DISCO_FP64, images=1, nu=0.35, image_split=0,
-                 max_atoms=0):
+                 max_atoms=0, image_min=0):
         self._lib = C.cuda_lib()
-        o = options(precision, images, nu, image_split)
+        o = options(precision, images, nu, image_split, image_min=image_min)
         arr, keep = loop_array(loops)
         b = (ctypes.c_double * 3)(*[float(v) for v in box])
         h = ctypes.c_void_p()
@@ -256,6 +257,7 @@ def sample_array(workloads, us=None, device_ptrs=None):
         d.nloops = len(w.loops)
         d.images = w.images
         d.box = C.D3(*w.box)
+        d.image_min = getattr(w, "image_min", 0)
     return arr, keep
 
 

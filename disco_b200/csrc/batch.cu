@@ -31,7 +31,7 @@ struct SampleDev {
     const Chunk* chunks;
     const LinePiece* pieces64;      // FP32 line form: FP64 pieces for the near-cut pass
     const LineSeg* segs64;
-    int32_t nchunks, images, nimg, pad;
+    int32_t nchunks, images, nimg, image_min;
     double Lx, Ly, Lz;
 };
 
@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
         }
         fa.images = sd.images;
         fa.nimg = sd.nimg;
+        fa.image_min = sd.image_min;
         fa.Lx = sd.Lx; fa.Ly = sd.Ly; fa.Lz = sd.Lz;
         fa.cJ = b.cJ; fa.cK = b.cK; fa.c2 = b.c2;
         fa.near_h = b.near_h; fa.near_r = b.near_r;
@@ -272,6 +273,7 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
     for (int s = 0; s < nsamples; ++s) {
         const disco_sample& sm = samples[s];
         if (sm.images < 0 || sm.images > 8) return bfail(DISCO_EINVAL, "sample images must be in 0..8");
+        if (sm.image_min < 0 || sm.image_min > sm.images) return bfail(DISCO_EINVAL, "sample image_min out of range");
         if (!(sm.box[0] > 0.) || !(sm.box[1] > 0.) || !(sm.box[2] > 0.)) return bfail(DISCO_EINVAL, "bad box");
         if (sm.atoms.n < 0 || (sm.atoms.n > 0 && (!sm.atoms.x || !sm.atoms.y || !sm.atoms.z ||
                                                   !sm.atoms.ux || !sm.atoms.uy || !sm.atoms.uz)))
@@ -316,6 +318,7 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
             sdev[s].n = sm.atoms.n;
             sdev[s].images = sm.images;
             sdev[s].nimg = W * W * W;
+            sdev[s].image_min = sm.image_min;
             sdev[s].Lx = sm.box[0]; sdev[s].Ly = sm.box[1]; sdev[s].Lz = sm.box[2];
             sdev[s].nchunks = (int32_t)T.chunks.size();
             if (T.chunks.empty()) continue;
@@ -328,7 +331,8 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
             aux_off[s] = T.aux_pieces ? base + T.aux_pieces : 0;
             aux_segs[s] = T.aux_segs ? base + T.aux_segs : 0;
             for (const Chunk& c : T.chunks) max_stage = std::max(max_stage, c.bytes);
-            work[s] = (double)(T.n_segments + T.n_loopons) * sdev[s].nimg;
+            const int inner = sm.image_min > 0 ? 2 * sm.image_min - 1 : 0;
+            work[s] = (double)(T.n_segments + T.n_loopons) * (sdev[s].nimg - inner * inner * inner);
             p->stats.n_segments += T.n_segments;
             p->stats.n_loopons += T.n_loopons;
             evals += work[s] * (double)sm.atoms.n;

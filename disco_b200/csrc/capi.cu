@@ -69,6 +69,7 @@ int check_options(const disco_options& o)
     if (o.precision != DISCO_FP64 && o.precision != DISCO_FP32C)
         return fail(DISCO_EINVAL, "precision must be DISCO_FP64 or DISCO_FP32C");
     if (o.images < 0 || o.images > 8) return fail(DISCO_EINVAL, "images must be in 0..8");
+    if (o.image_min < 0 || o.image_min > o.images) return fail(DISCO_EINVAL, "image_min must be in 0..images");
     if (!(o.nu > -1.0 && o.nu < 0.5)) return fail(DISCO_EINVAL, "nu must be in (-1, 0.5)");
     if (!(o.near_plane >= 0.0) || !(o.near_rim >= 0.0))
         return fail(DISCO_EINVAL, "near_plane and near_rim must be >= 0");
@@ -209,7 +210,11 @@ int disco_b200_plan_create(const disco_loop* loops, int32_t nloops, const double
                            cudaMemcpyHostToDevice);
         if (e != cudaSuccess) { free_plan(p); return cuda_fail(e, "loop table upload"); }
     }
-    p->stats.evals_per_atom = (double)(p->stats.n_segments + p->stats.n_loopons) * p->nimg;
+    {
+        const int inner = o.image_min > 0 ? 2 * o.image_min - 1 : 0;
+        p->stats.n_images = p->nimg - inner * inner * inner;
+    }
+    p->stats.evals_per_atom = (double)(p->stats.n_segments + p->stats.n_loopons) * p->stats.n_images;
     e = cudaMalloc(&p->d_status, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(int));
     if (e != cudaSuccess) { free_plan(p); return cuda_fail(e, "status word"); }
@@ -239,6 +244,7 @@ int disco_b200_plan_execute(disco_plan* p, const disco_atoms* a, void* stream)
         fa.resident = T.resident ? 1 : 0;
         fa.images = p->opt.images;
         fa.nimg = p->nimg;
+        fa.image_min = p->opt.image_min;
         fa.Lx = p->box[0]; fa.Ly = p->box[1]; fa.Lz = p->box[2];
         const double pi = 3.14159265358979323846;
         const double c3 = 1.0 / (8.0 * pi * (1.0 - p->opt.nu));      // Code/barnett.hpp:51

@@ -112,6 +112,8 @@ struct FieldArgs {
     uint32_t stage_bytes;     // shared-memory bytes of one stage buffer
     int32_t resident;         // one chunk, loaded once per CTA
     int32_t images, nimg;     // image range and (2 images + 1)^3
+    int32_t image_min;        // skip images with max(|i|,|j|,|k|) < image_min
+    int32_t pad_;
     double Lx, Ly, Lz;
     double cJ, cK;            // line: c3 - 1/(4 pi), c3 = 1 / (8 pi (1 - nu))
     double c2;                // loopon: 1 - 2 nu

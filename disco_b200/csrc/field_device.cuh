@@ -19,8 +19,11 @@ constexpr uint32_t kResidentMax = 110u * 1024u;
 constexpr uint32_t kStageMax = 48u * 1024u;
 constexpr uint32_t kSmemHeader = 128;      // mbarriers at the start of shared memory
 
-__device__ __forceinline__ void image_shift(int img, int images, double Lx, double Ly, double Lz,
-                                            double& sx, double& sy, double& sz)
+// Image img of the (2 images + 1)^3 cube, kk fastest (Code/backend_cpu.cpp:51-53).
+// Returns false for an image inside the inner cube max(|i|,|j|,|k|) < image_min
+// (image_min = 2 keeps only the far shells 2 <= max|n| <= images).
+__device__ __forceinline__ bool image_shift(int img, int images, int image_min, double Lx, double Ly,
+                                            double Lz, double& sx, double& sy, double& sz)
 {
     const int W = 2 * images + 1;
     const int ii = img / (W * W) - images;
@@ -30,6 +33,8 @@ __device__ __forceinline__ void image_shift(int img, int images, double Lx, doub
     sx = Lx * ii;
     sy = Ly * jj;
     sz = Lz * kk;
+    const int m = max(abs(ii), max(abs(jj), abs(kk)));
+    return m >= image_min;
 }
 
 // 1/y for a positive normal y: the hardware approximation (rcp.approx.ftz.f64)
@@ -204,7 +209,7 @@ struct LineFp64 {
             const LinePiece& pc = pieces[p];
             for (int img = split; img < a.nimg; img += S) {
                 double sx, sy, sz;
-                image_shift(img, a.images, a.Lx, a.Ly, a.Lz, sx, sy, sz);
+                if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
                 line_piece_fp64(pc, recs + pc.rec, px - sx, py - sy, pz - sz, a.cJ, a.cK, acc.x, acc.y, acc.z);
             }
         }
@@ -225,7 +230,7 @@ struct LooponFp64 {
             const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
             for (int img = split; img < a.nimg; img += S) {
                 double sx, sy, sz;
-                image_shift(img, a.images, a.Lx, a.Ly, a.Lz, sx, sy, sz);
+                if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
                 loopon_piece_fp64(pc, recs + pc.rec, qx - sx, qy - sy, qz - sz, a.c2, acc.x, acc.y, acc.z);
             }
         }

@@ -158,7 +158,7 @@ struct LineFp32 {
             const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
             for (int img = split; img < a.nimg; img += S) {
                 double sx, sy, sz;
-                image_shift(img, a.images, a.Lx, a.Ly, a.Lz, sx, sy, sz);
+                if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
                 const float Px = (float)(qx - sx), Py = (float)(qy - sy), Pz = (float)(qz - sz);
                 if (near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) continue;
                 float fx = 0.0f, fy = 0.0f, fz = 0.0f;
@@ -183,7 +183,7 @@ struct LineNearFp64 {
             const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
             for (int img = split; img < a.nimg; img += S) {
                 double sx, sy, sz;
-                image_shift(img, a.images, a.Lx, a.Ly, a.Lz, sx, sy, sz);
+                if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
                 const float Px = (float)(qx - sx), Py = (float)(qy - sy), Pz = (float)(qz - sz);
                 if (!near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) continue;
                 const LinePiece& p64 = a.pieces64[pc.piece64];
@@ -209,7 +209,7 @@ struct LooponFp32 {
             const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
             for (int img = split; img < a.nimg; img += S) {
                 double sx, sy, sz;
-                image_shift(img, a.images, a.Lx, a.Ly, a.Lz, sx, sy, sz);
+                if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
                 float fx = 0.0f, fy = 0.0f, fz = 0.0f;
                 loopon_piece_fp32(pc, recs + pc.rec, (float)(qx - sx), (float)(qy - sy), (float)(qz - sz),
                                   c2, fx, fy, fz);

@@ -26,17 +26,11 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "mlp.cuh"
 #include "tcgen05.cuh"
 
 namespace disco {
 namespace mlp {
-
-constexpr int kIn = 16, kHid = 128, kOut = 16;       // padded widths
-constexpr int kInReal = 14, kOutReal = 3;
-// parameter offsets (floats): W1 [128 x 16], b1, W2 [128 x 128], b2, W3, b3, W4 [16 x 128], b4
-constexpr int oW1 = 0, ob1 = oW1 + kHid * kIn, oW2 = ob1 + kHid, ob2 = oW2 + kHid * kHid;
-constexpr int oW3 = ob2 + kHid, ob3 = oW3 + kHid * kHid, oW4 = ob3 + kHid, ob4 = oW4 + kOut * kHid;
-constexpr int kParams = ob4 + kOut;                  // 37 264
 
 enum { kF32 = 0, kBF16 = 1 };
 enum { EPI_STORE = 0, EPI_SILU = 1, EPI_DSILU = 2, EPI_ATOMIC = 3, EPI_ATOMIC_T = 4 };
@@ -96,7 +90,6 @@ __device__ __forceinline__ void load_tile(const Operand& o, __nv_bfloat16* smem,
     }
 }
 
-__device__ __forceinline__ float sigmoidf_fast(float x) { return 1.0f / (1.0f + __expf(-x)); }
 
 template <int NT>
 __global__ void __launch_bounds__(kThreads) gemm_kernel(const GemmArgs g)
@@ -167,13 +160,12 @@ __global__ void __launch_bounds__(kThreads) gemm_kernel(const GemmArgs g)
                 case EPI_SILU: {
                     if (g.bias) x += g.bias[col];
                     g.C[row * g.ldc + col] = x;
-                    g.H[row * g.ldh + col] = __float2bfloat16_rn(x * sigmoidf_fast(x));
+                    g.H[row * g.ldh + col] = __float2bfloat16_rn(silu_half(0.5f * x));
                     break;
                 }
                 case EPI_DSILU: {
                     const float p = g.pre[row * g.ldp + col];
-                    const float s = sigmoidf_fast(p);
-                    const float d = x * s * (1.0f + p * (1.0f - s));
+                    const float d = x * dsilu(p);
                     g.C[row * g.ldc + col] = d;
                     g.H[row * g.ldh + col] = __float2bfloat16_rn(d);
                     break;
@@ -254,18 +246,6 @@ __global__ void adam_kernel(float* p, float* g, float* m, float* v, int n, float
 
 // ---- host ---------------------------------------------------------------------------------
 
-struct disco_mlp {
-    float* params = nullptr;   // FP32 master weights (device)
-    float* grads = nullptr;
-    float* m = nullptr;
-    float* v = nullptr;
-    float* loss = nullptr;     // device scalar
-    int64_t cap = 0;           // rows of the workspace below
-    float *pre1 = nullptr, *pre2 = nullptr, *pre3 = nullptr, *y = nullptr, *dy = nullptr, *dpre = nullptr;
-    __nv_bfloat16 *h1 = nullptr, *h2 = nullptr, *h3 = nullptr, *dpre_h = nullptr;
-    int64_t step = 0;
-    int* status = nullptr;
-};
 
 namespace {
 
@@ -322,6 +302,7 @@ void free_mlp(disco_mlp* p)
     __nv_bfloat16* hs[] = { p->h1, p->h2, p->h3, p->dpre_h };
     for (auto* h : hs) if (h) cudaFree(h);
     if (p->status) cudaFree(p->status);
+    if (p->packed) cudaFree(p->packed);
     delete p;
 }
 

@@ -93,6 +93,30 @@ def quadrupole(cells=40, a0=2.855, radius=30.0, eps=0.0365, nu=0.29, images=1, d
                     (cells, cells, cells), geom=geom)
 
 
+def _fcc_glide_loop(rng, kind, cells, a0, da, chords):
+    """One glide loop of the fcc_random distribution: a random {111} plane, b =
+    a0/2<110> in it, centre uniform in the box (snapped to a mid-plane)."""
+    L = cells * a0
+    n = _N111[rng.integers(len(_N111))]
+    ms = _in_plane_110(n)
+    m = ms[rng.integers(len(ms))]
+    c = rng.uniform(-L / 2, L / 2, size=3)
+    cs, _ = G.snap(c, n, a0, cells, cells, cells, G.FCC)
+    if kind == "circle":
+        R = rng.uniform(10.0, 40.0)
+        lp = G.Loop.circle(da, R, cs, m, n, a0)
+        P = lp.polyline(G.circle_eps_for_chords(R, chords))
+    elif kind == "hexagon":
+        R = rng.uniform(15.0, 35.0)
+        lp = G.Loop.polygon(da, G.regular_polygon(6, R, m, n), 0.0, cs, m, n, a0)
+        P = lp.polyline(0.01)
+    else:
+        s1, s2 = rng.uniform(20.0, 60.0, size=2)
+        lp = G.Loop.rectangle(da, s1 / 2, s2 / 2, 0.0, cs, m, n, a0)
+        P = lp.polyline(0.01)
+    return lp, lp.line_data(vertices=P)
+
+
 def fcc_random(cells=150, a0=3.615, nu=0.34, images=2, seed=2, n_circles=32, n_hex=16, n_rect=16,
                chords=48, da=1.0):
     """64 random shear loops in an FCC box, line method."""
@@ -102,27 +126,19 @@ def fcc_random(cells=150, a0=3.615, nu=0.34, images=2, seed=2, n_circles=32, n_h
     loops, geom = [], []
     kinds = ["circle"] * n_circles + ["hexagon"] * n_hex + ["rectangle"] * n_rect
     for kind in kinds:
-        n = _N111[rng.integers(len(_N111))]
-        ms = _in_plane_110(n)
-        m = ms[rng.integers(len(ms))]
-        c = rng.uniform(-L / 2, L / 2, size=3)
-        cs, _ = G.snap(c, n, a0, cells, cells, cells, G.FCC)
-        if kind == "circle":
-            R = rng.uniform(10.0, 40.0)
-            lp = G.Loop.circle(da, R, cs, m, n, a0)
-            P = lp.polyline(G.circle_eps_for_chords(R, chords))
-        elif kind == "hexagon":
-            R = rng.uniform(15.0, 35.0)
-            lp = G.Loop.polygon(da, G.regular_polygon(6, R, m, n), 0.0, cs, m, n, a0)
-            P = lp.polyline(0.01)
-        else:
-            s1, s2 = rng.uniform(20.0, 60.0, size=2)
-            lp = G.Loop.rectangle(da, s1 / 2, s2 / 2, 0.0, cs, m, n, a0)
-            P = lp.polyline(0.01)
+        lp, ld = _fcc_glide_loop(rng, kind, cells, a0, da, chords)
         geom.append(lp)
-        loops.append(lp.line_data(vertices=P))
+        loops.append(ld)
     return Workload("fcc_random", x, y, z, loops, (L, L, L), images, nu, "line", G.FCC, a0,
                     (cells, cells, cells), geom=geom)
+
+
+def fcc_random_loops(count, seed, cells=150, a0=3.615, chords=48, da=1.0):
+    """`count` loops drawn from the fcc_random distribution (kinds in its
+    proportions: half circles, a quarter hexagons, a quarter rectangles)."""
+    rng = np.random.default_rng(seed)
+    kinds = rng.choice(["circle", "circle", "hexagon", "rectangle"], size=count)
+    return [_fcc_glide_loop(rng, k, cells, a0, da, chords)[1] for k in kinds]
 
 
 def bcc_prismatic(cells=60, a0=3.165, nu=0.28, images=1, seed=3, n_inter=8, n_vac=8, da=1.0,

@@ -111,7 +111,8 @@ typedef struct {
     double  near_rim;
     int32_t stage_kb;          /* shared-memory stage of the streamed tables, KB;
                                   0 = automatic (resident up to 110 KB, else 48)  */
-    int32_t reserved;
+    int32_t image_min;         /* skip the images with max(|i|,|j|,|k|) < image_min:
+                                  2 sums only the far shells 2 <= max|n| <= images */
 } disco_options;
 
 /* Phase timings, seconds: Code/backend.hpp:36-39 (BackendTiming).
@@ -183,6 +184,8 @@ typedef struct {
     int32_t nloops;
     int32_t images;
     double box[3];
+    int32_t image_min;        /* as disco_options.image_min, per sample */
+    int32_t reserved;
 } disco_sample;
 
 typedef struct disco_batch_plan disco_batch_plan;
@@ -229,6 +232,83 @@ int disco_b200_mlp_adam(disco_mlp *m, float lr, float beta1, float beta2, float 
                         float weight_decay, void *stream);
 /* waits for the device and reports a bounded wait of an MLP kernel that gave up */
 int disco_b200_mlp_status(disco_mlp *m);
+
+/* ---- learned far-image surrogate: features, inference, learned displacement ----------
+ * The network stands in for a line loop's field summed over the far image shells
+ * image_min <= max(|i|,|j|,|k|) <= images.  Its 14 features for atom r and loop
+ * (centre c, area A, largest vertex radius rho_max, unit normal n, Burgers vector b;
+ * box L = (Lx, Ly, Lz), Lref = (Lx Ly Lz)^(1/3)):
+ *     0-2  (r-c)_x / Lx, (r-c)_y / Ly, (r-c)_z / Lz   position relative to the loop
+ *          centre over the box lengths (loop-centred frame, box axes, in (-1, 1))
+ *     3    sqrt(A / pi) / Lref          loop radius over box edge
+ *     4-6  n                            plane normal
+ *     7-9  b / |b|                      Burgers vector direction
+ *     10   Ly / Lx - 1, 11 Lz / Lx - 1  box aspect ratios
+ *     12   rho_max / sqrt(A / pi) - 1   shape (0 for a circle)
+ *     13   (b / |b|) . n                0 for a glide loop
+ * each entering as (raw - mu) * inv_sd (features 14, 15 are zero padding).  The
+ * network's outputs 0-2 times gain = out_scale |b| A / Lref^2 are the loop's
+ * displacement (A, box axes) summed over those shells. */
+typedef struct {
+    float mu[16];
+    float inv_sd[16];
+    float out_scale;
+    int32_t images;           /* the shells the network was trained for */
+    int32_t image_min;
+    int32_t reserved;
+} disco_far_norm;
+
+/* Features of every (loop, atom) pair, loop-major: X[(l n + i) 16 + k] (DEVICE,
+ * FP32).  norm NULL: raw features (mu 0, inv_sd 1) and gain without out_scale.
+ * gain: DEVICE array of nloops floats, or NULL.  Line loops only. */
+int disco_b200_far_features(const disco_atoms *device_atoms, const disco_loop *loops, int32_t nloops,
+                            const double box[3], const disco_far_norm *norm, float *X, float *gain,
+                            void *stream);
+
+/* The network's far-shell displacement of the loops loop_sel[0..nsel) (host
+ * indices; NULL = all nloops) at every atom, in one fused tcgen05 kernel:
+ * features, four layers and the gain.  per_loop NULL: added into the atoms'
+ * ux/uy/uz; else written to per_loop[(j 3 + c) n + i] (DEVICE, FP32) for the
+ * j-th selected loop.  One call at a time per network. */
+int disco_b200_far_apply(disco_mlp *m, const disco_far_norm *norm, const disco_atoms *device_atoms,
+                         const disco_loop *loops, int32_t nloops, const double box[3],
+                         const int32_t *loop_sel, int32_t nsel, float *per_loop, void *stream);
+
+typedef struct {
+    int32_t precision;        /* near shell and fallback loops: DISCO_FP32C or DISCO_FP64 */
+    int32_t check_precision;  /* exact far shells on the check subsample              */
+    double  nu;
+    double  check_fraction;   /* share of the atoms re-checked every call (0.01)      */
+    double  tol_loop;         /* a loop whose network error exceeds this on the
+                                 subsample is summed exactly (1e-3 A)                */
+    double  tol_total;        /* further loops fall back, largest error first, until
+                                 the subsample's total far-shell error is within this */
+    uint64_t seed;            /* subsample: one atom drawn in each of n_check equal
+                                 index strata                                        */
+} disco_learned_options;
+
+typedef struct {
+    int64_t n_check;          /* atoms in the check subsample                          */
+    int32_t n_fallback;       /* loops whose far shells were summed exactly            */
+    int32_t launches;         /* kernels this call launched                            */
+    double  check_max;        /* max |du| of the network's part on the subsample, A   */
+    double  check_rms;
+    double  worst_loop;       /* largest per-loop max |du| before any fallback, A      */
+    double  t_check, t_near, t_far, t_fallback;   /* device seconds of each phase      */
+    double *loop_err;         /* caller array of nloops or NULL: per-loop max |du|     */
+    int32_t *fallback;        /* caller array of nloops or NULL: 1 = summed exactly    */
+} disco_learned_report;
+
+/* Learned displacement: u += the exact field of every loop over the near images
+ * max|n| < norm->image_min (opt->precision) plus the network's far shells
+ * image_min <= max|n| <= norm->images, with the exact far-shell sum
+ * (opt->check_precision) recomputed per loop on a random atom subsample every
+ * call and replacing the network for the loops that miss the tolerances.
+ * DEVICE atoms; the call returns when the work is done. */
+int disco_b200_learned_displace(disco_mlp *m, const disco_far_norm *norm, const disco_atoms *device_atoms,
+                                const disco_loop *loops, int32_t nloops, const double box[3],
+                                const disco_learned_options *opt, disco_learned_report *report,
+                                void *stream);
 
 /* ---- prismatic loops: slab selection and stream compaction ------------------------ */
 

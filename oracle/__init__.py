@@ -74,6 +74,10 @@ def _load(path):
             lib.oracle_displace.restype = c_int
             lib.oracle_displace.argtypes = [POINTER(C.DiscoAtoms), POINTER(C.DiscoLoop), c_int,
                                             POINTER(c_double), c_int, c_double, c_int, c_void_p]
+            lib.oracle_displace_shells.restype = c_int
+            lib.oracle_displace_shells.argtypes = [POINTER(C.DiscoAtoms), POINTER(C.DiscoLoop), c_int,
+                                                   POINTER(c_double), c_int, c_int, c_double, c_int,
+                                                   c_void_p]
             lib.oracle_prismatic.restype = c_int
             lib.oracle_prismatic.argtypes = [c_void_p, c_void_p, c_void_p, c_int64,
                                              POINTER(C.DiscoSlabLoop), c_int32, POINTER(c_double),
@@ -116,15 +120,17 @@ def _atoms(x, y, z):
     return a, (x, y, z), u
 
 
-def displace(x, y, z, loops, box, images=1, nu=0.35, threads=0, nofma=False, loop_sec=None):
-    """oracle_displace: (ux, uy, uz) of every loop over images -images..images."""
+def displace(x, y, z, loops, box, images=1, nu=0.35, threads=0, nofma=False, loop_sec=None,
+             image_min=0):
+    """oracle_displace: (ux, uy, uz) of every loop over images -images..images
+    (image_min > 0: only the shells image_min <= max|n| <= images)."""
     from disco_b200.backend import loop_array
     lib = oracle_lib(nofma)
     a, keep_x, u = _atoms(x, y, z)
     arr, keep = loop_array(loops)
     ls = np.zeros(max(1, len(loops)))
-    st = lib.oracle_displace(ctypes.byref(a), arr, len(loops), _box(box), images, nu, threads,
-                             ls.ctypes.data)
+    st = lib.oracle_displace_shells(ctypes.byref(a), arr, len(loops), _box(box), images, image_min, nu,
+                                    threads, ls.ctypes.data)
     assert st == 0
     if loop_sec is not None:
         loop_sec[:] = ls[:len(loops)]

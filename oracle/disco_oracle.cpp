@@ -19,7 +19,9 @@
 // and with -ffp-contract=off, the build the atom-set comparisons use.
 // =============================================================================
 
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -191,9 +193,11 @@ void oracle_kroupa_pair(double rx, double ry, double rz, const disco_loop_phys* 
 
 // Code/backend_cpu.cpp:28-99: loop by loop; per loop an OpenMP loop over atoms,
 // images ii, jj, kk in -images..images (kk fastest), each loop's partial added
-// to the atom.  threads <= 0 keeps the OpenMP default.
-int oracle_displace(const disco_atoms* atoms, const disco_loop* loops, int nloops,
-                    const double box[3], int images, double nu, int threads, double* loop_sec)
+// to the atom.  threads <= 0 keeps the OpenMP default.  Images with
+// max(|ii|,|jj|,|kk|) < image_min are skipped (image_min 0: the reference's sum).
+int oracle_displace_shells(const disco_atoms* atoms, const disco_loop* loops, int nloops,
+                           const double box[3], int images, int image_min, double nu, int threads,
+                           double* loop_sec)
 {
     if (threads > 0) omp_set_num_threads(threads);
     const int64_t nbAtoms = atoms->n;
@@ -216,6 +220,7 @@ int oracle_displace(const disco_atoms* atoms, const disco_loop* loops, int nloop
                 for (int ii = -I; ii <= I; ii++)
                 for (int jj = -I; jj <= I; jj++)
                 for (int kk = -I; kk <= I; kk++)
+                    if (std::max(std::abs(ii), std::max(std::abs(jj), std::abs(kk))) >= image_min)
                     barnett_loop(atoms->x[a] - dx*ii, atoms->y[a] - dy*jj, atoms->z[a] - dz*kk,
                                  lp.vx, lp.vy, lp.vz, nv, lp.cx, lp.cy, lp.cz, bx, by, bz,
                                  c3, cJ, c3, dux, duy, duz);
@@ -237,6 +242,7 @@ int oracle_displace(const disco_atoms* atoms, const disco_loop* loops, int nloop
                 for (int ii = -I; ii <= I; ii++) {
                 for (int jj = -I; jj <= I; jj++) {
                 for (int kk = -I; kk <= I; kk++) {
+                    if (std::max(std::abs(ii), std::max(std::abs(jj), std::abs(kk))) < image_min) continue;
                     const double delta_x = dx * ii;
                     const double delta_y = dy * jj;
                     const double delta_z = dz * kk;
@@ -253,6 +259,12 @@ int oracle_displace(const disco_atoms* atoms, const disco_loop* loops, int nloop
         if (loop_sec) loop_sec[l] = omp_get_wtime() - t0;
     }
     return DISCO_OK;
+}
+
+int oracle_displace(const disco_atoms* atoms, const disco_loop* loops, int nloops,
+                    const double box[3], int images, double nu, int threads, double* loop_sec)
+{
+    return oracle_displace_shells(atoms, loops, nloops, box, images, 0, nu, threads, loop_sec);
 }
 
 // One slab (Code/prismatic.cpp:36-74): fills info and appends atoms/side.

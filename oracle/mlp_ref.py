@@ -47,6 +47,15 @@ def dsilu(x):
     return s * (1.0 + x * (1.0 - s))
 
 
+def forward_f64(p, X):
+    """The network without any BF16 rounding (what the weights mean)."""
+    P = unpack(p)
+    h = np.asarray(X, dtype=np.float64)
+    for W, b in (("W1", "b1"), ("W2", "b2"), ("W3", "b3")):
+        h = silu(h @ P[W].T + P[b])
+    return h @ P["W4"].T + P["b4"]
+
+
 def forward(p, X):
     P = unpack(p)
     x0 = bf16(X)

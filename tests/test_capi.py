@@ -84,3 +84,36 @@ def test_no_device_reports_enodev():
     assert e.value.status == C.DISCO_ENODEV
     buf = ctypes.create_string_buffer(64)
     assert C.cuda_lib().disco_b200_device_info(buf, 64) == C.DISCO_ENODEV
+
+
+def test_ctypes_structures_match_the_header(tmp_path):
+    """Every structure of include/disco_b200.h has the size and field offsets of
+    its ctypes mirror (a C program compiled against the header prints them)."""
+    import ctypes
+    import shutil
+    import subprocess
+    from disco_b200 import _capi as C
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    pairs = {"disco_atoms": C.DiscoAtoms, "disco_loop_phys": C.DiscoLoopPhys, "disco_loop": C.DiscoLoop,
+             "disco_options": C.DiscoOptions, "disco_sample": C.DiscoSample, "disco_timing": C.DiscoTiming,
+             "disco_plan_stats": C.DiscoPlanStats, "disco_slab_loop": C.DiscoSlabLoop,
+             "disco_slab_info": C.DiscoSlabInfo, "disco_copy": C.DiscoCopy, "disco_far_norm": C.DiscoFarNorm,
+             "disco_learned_options": C.DiscoLearnedOptions, "disco_learned_report": C.DiscoLearnedReport}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "disco_b200.h"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-std=c11", "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in pairs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f in py._fields_:
+            assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])

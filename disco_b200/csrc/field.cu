@@ -174,3 +174,42 @@ int launch_field(const FieldArgs& a, int kind, bool fp32, int sm_count, int thre
 }
 
 } // namespace disco
+
+// ---- self-test of the kernels' own FP64 math routines -------------------------------------
+
+namespace {
+
+__global__ void math_check_kernel(int fn, const double* x, double* y, int64_t n)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double v = x[i];
+        double r;
+        switch (fn) {
+        case 0: r = disco::rsqrt_nr(v); break;
+        case 1: r = disco::rcp_nr(v); break;
+        case 2: r = 2.0 * disco::half_j0_series<8>(v); break;
+        case 3: r = 2.0 * disco::half_j0_series<6>(v); break;
+        default: r = 2.0 * disco::half_j0_series<4>(v); break;
+        }
+        y[i] = r;
+    }
+}
+
+} // namespace
+
+extern "C" int disco_b200_math_check(int32_t fn, const double* x, double* y, int64_t n, void* stream)
+{
+    if (fn < 0 || fn > 4 || n < 0 || (n > 0 && (!x || !y))) {
+        disco::set_last_error("math_check: bad argument");
+        return DISCO_EINVAL;
+    }
+    if (n == 0) return DISCO_OK;
+    const int grid = (int)std::min<int64_t>((n + 255) / 256, 4096);
+    math_check_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(fn, x, y, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        disco::set_last_error(std::string("math_check: ") + cudaGetErrorString(e));
+        return DISCO_ECUDA;
+    }
+    return DISCO_OK;
+}

@@ -24,7 +24,7 @@ constexpr int kLooponKind = 1;
 
 // ---- FP64 line method (Code/barnett.hpp:44-107) --------------------------------
 struct alignas(16) LinePiece {
-    double ax, ay, az;   // vertex before the piece's first segment
+    double ax, ay, az;   // vertex before the piece's first segment, minus the apex
     double cx, cy, cz;   // fan apex (loop centre)
     double bx, by, bz;   // Burgers vector (phys.b * m)
     double rho;          // largest |vertex - apex| over the piece's vertices
@@ -33,12 +33,14 @@ struct alignas(16) LinePiece {
     int32_t rec;         // first segment record, index into the chunk's records
 };
 struct alignas(16) LineSeg {
-    double vx, vy, vz;   // end vertex B of segment A -> B
+    double vx, vy, vz;   // end vertex B of segment A -> B, minus the apex
     double len;          // |B - A|
     double tx, ty, tz;   // unit tangent (B - A) / |B - A| (0 for a null segment)
     double wx, wy, wz;   // w = b x t
+    double nx, ny, nz;   // (A - apex) x (B - apex)
+    double pad;
 };
-static_assert(sizeof(LinePiece) == 96 && sizeof(LineSeg) == 80, "line table layout");
+static_assert(sizeof(LinePiece) == 96 && sizeof(LineSeg) == 112, "line table layout");
 
 // ---- FP64 loopon method (Code/kroupa.hpp:52-73) ---------------------------------
 struct alignas(16) LooponPiece {
@@ -77,9 +79,10 @@ struct alignas(16) LineSegF {
     float vx, vy, vz, len;   // end vertex - centre, length
     float tx, ty, tz;        // unit tangent
     float wx, wy, wz;        // b x t
-    float pad0, pad1;        // 48 B
+    float nx, ny, nz;        // (start - centre) x (end - centre)
+    float pad0, pad1, pad2;  // 64 B
 };
-static_assert(sizeof(LinePieceF) == 80 && sizeof(LineSegF) == 48, "fp32 line table layout");
+static_assert(sizeof(LinePieceF) == 80 && sizeof(LineSegF) == 64, "fp32 line table layout");
 
 struct alignas(16) LooponPieceF {
     double cx, cy, cz;      // reference point (FP64)

@@ -48,52 +48,74 @@ __device__ __forceinline__ double rcp_nr(double y)
     return fma(r0, fma(e, e, e), r0);
 }
 
-// Largest t = L/(RA+RB) for which the 8-term series of 2 atanh(t) is exact to
-// the double rounding: its remainder relative to the sum is below t^16/17.
-constexpr double kSeriesTau = 0.11;
-
-// J0 = ln((S+L)/(S-L)) = 2 atanh(t), t = L/S:  2 t (1 + t^2/3 + ... + t^14/15).
-__device__ __forceinline__ double j0_series(double t)
+// 1/sqrt(x) for a positive normal x: the hardware approximation
+// (rsqrt.approx.ftz.f64) refined by one cubic Householder step of
+// f(r) = 1/r^2 - x:  r = r0 (1 + e/2 + 3 e^2/8), e = 1 - x r0^2.
+__device__ __forceinline__ double rsqrt_nr(double x)
 {
-    const double t2 = t * t;
-    double p = 1.0 / 15.0;
-    p = fma(p, t2, 1.0 / 13.0);
-    p = fma(p, t2, 1.0 / 11.0);
-    p = fma(p, t2, 1.0 / 9.0);
-    p = fma(p, t2, 1.0 / 7.0);
-    p = fma(p, t2, 1.0 / 5.0);
-    p = fma(p, t2, 1.0 / 3.0);
-    p = fma(p, t2, 1.0);
-    return 2.0 * t * p;
+    double r0;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r0) : "d"(x));
+    const double e = fma(-(x * r0), r0, 1.0);
+    return fma(r0 * e, fma(0.375, e, 0.5), r0);
 }
 
-// The segment loop of one line piece.  FAR: every segment of the piece is far
-// enough from P (for every lane of the warp) that J0 comes from the series.
-template <bool FAR>
-__device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, double Px, double Py, double Pz,
+// J0 = ln((S+L)/(S-L)) = 2 atanh(t), t = L/S, as the series
+// 2 t (1 + t^2/3 + ... + t^(2N-2)/(2N-1)); line_terms<N> returns the half,
+// t (1 + ...).  Its remainder relative to the sum is below t^(2N)/(2N+1), under
+// 2^-53 for t <= 0.012 (N = 4), 0.054 (N = 6), 0.11 (N = 8).
+template <int N>
+__device__ __forceinline__ double half_j0_series(double t)
+{
+    const double t2 = t * t;
+    double p = 1.0 / (2 * N - 1);
+#pragma unroll
+    for (int k = N - 2; k >= 0; --k) p = fma(p, t2, 1.0 / (2 * k + 1));
+    return t * p;
+}
+
+// Series tiers: the warp takes the shortest series valid for all its lanes;
+// tier 0 is the logarithm.
+constexpr double kSeriesT4 = 0.012, kSeriesT6 = 0.054, kSeriesT8 = 0.11;
+
+// Tier of a lane whose segments all have t <= lmax / gap2 (gap2 > 0).
+__device__ __forceinline__ unsigned series_tier(double lmax, double gap2)
+{
+    return lmax <= kSeriesT4 * gap2 ? 3u : lmax <= kSeriesT6 * gap2 ? 2u : lmax <= kSeriesT8 * gap2 ? 1u : 0u;
+}
+
+// The segment loop of one line piece.  NS = 0: J0 from the logarithm; NS > 0:
+// every segment is far enough from P (for every lane of the warp) that the
+// NS-term series is exact.  The solid angle accumulates as the argument of
+// the product of (la lb)(1 + e.ha + e.hb + ha.hb) + i (la lb) e.(ha x hb) over
+// the fan triangles (Van Oosterom-Strackee on unnormalised vectors; the
+// positive factor la lb does not change the argument), renormalised every 16
+// segments.  With d = a - sA t: |d|^2 = |a|^2 - sA^2 and d.w = a.w (w = b x t
+// is orthogonal to t), so d is never formed; its term -al d enters as
+// -al a + al sA t.  cK is folded into d.w, 2 cJ into the J0 factor.
+template <int NS>
+__device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, double rx, double ry, double rz,
                                               double ex, double ey, double ez, double ax, double ay, double az,
                                               double cJ, double cK, double& zr, double& zi,
                                               double& lx, double& ly, double& lz)
 {
-    const double la2 = ax * ax + ay * ay + az * az;
-    double ila = rsqrt(la2);
+    const double c2J = 2.0 * cJ;
+    double la2 = ax * ax + ay * ay + az * az;
+    double ila = rsqrt_nr(la2);
     double la = la2 * ila;
-    double hax = ax * ila, hay = ay * ila, haz = az * ila;
-    double ca = ex * hax + ey * hay + ez * haz;                 // e . a-hat
-    double qx = ey * haz - ez * hay, qy = ez * hax - ex * haz, qz = ex * hay - ey * hax;   // e x a-hat
+    double ea = ex * ax + ey * ay + ez * az;                            // e . a
+#pragma unroll 2
     for (int k = 0; k < nseg; ++k) {
         const LineSeg s = seg[k];
-        const double bx = s.vx - Px, by = s.vy - Py, bz = s.vz - Pz;
+        const double bx = s.vx + rx, by = s.vy + ry, bz = s.vz + rz;    // B - P
         const double lb2 = bx * bx + by * by + bz * bz;
-        const double ilb = rsqrt(lb2);
+        const double ilb = rsqrt_nr(lb2);
         const double lb = lb2 * ilb;
-        const double hbx = bx * ilb, hby = by * ilb, hbz = bz * ilb;
-        const double cb = ex * hbx + ey * hby + ez * hbz;
+        const double eb = ex * bx + ey * by + ez * bz;
 
-        // solid angle of triangle (apex, A, B): tan(Omega/2) = num / den on unit
-        // vectors (Code/barnett.hpp:69-72 divided by l1 la lb > 0)
-        const double den = 1.0 + ca + cb + (hax * hbx + hay * hby + haz * hbz);
-        const double num = qx * hbx + qy * hby + qz * hbz;
+        // solid angle of triangle (apex, A, B), Code/barnett.hpp:69-72 times l1 la lb;
+        // e.(a x b) = e.((A - apex) x (B - apex)) as e is along apex - P
+        const double den = fma(ea, lb, fma(eb, la, fma(la, lb, ax * bx + ay * by + az * bz)));
+        const double num = ex * s.nx + ey * s.ny + ez * s.nz;
         const double nzr = zr * den - zi * num;
         zi = zr * num + zi * den;
         zr = nzr;
@@ -101,27 +123,24 @@ __device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, doub
         // segment A -> B (Code/barnett.hpp:75-100)
         const double sA = ax * s.tx + ay * s.ty + az * s.tz;
         const double sB = sA + s.len;
-        const double dx = ax - sA * s.tx, dy = ay - sA * s.ty, dz = az - sA * s.tz;
-        const double d2 = dx * dx + dy * dy + dz * dz;
-        const double dw = dx * s.wx + dy * s.wy + dz * s.wz;
+        const double d2 = fma(-sA, sA, la2);
+        const double dw = cK * (ax * s.wx + ay * s.wy + az * s.wz);      // cK d.w
         const double sum = la + lb;
-        double J0;
-        if (FAR) J0 = j0_series(s.len * rcp_nr(sum));
-        else     J0 = log((sum + s.len) * rcp_nr(sum - s.len));
-        const double g = sB * ilb - sA * ila;                   // d^2 K0
-        const double q = d2 > 0.0 ? dw * rcp_nr(d2) : 0.0;
-        const double K1 = ila - ilb;
-        const double al = cK * q * g, be = cK * dw * K1, ga = cJ * J0;
-        lx += ga * s.wx - al * dx - be * s.tx;
-        ly += ga * s.wy - al * dy - be * s.ty;
-        lz += ga * s.wz - al * dz - be * s.tz;
+        double ga;
+        if (NS > 0) ga = c2J * half_j0_series<NS>(s.len * rcp_nr(sum));
+        else        ga = cJ * log((sum + s.len) * rcp_nr(sum - s.len));
+        const double g = sB * ilb - sA * ila;                           // d^2 K0
+        const double al = d2 > 0.0 ? dw * rcp_nr(d2) * g : 0.0;
+        const double be = dw * (ila - ilb);                             // cK d.w K1
+        const double c = fma(al, sA, -be);
+        lx = fma(c, s.tx, fma(-al, ax, fma(ga, s.wx, lx)));
+        ly = fma(c, s.ty, fma(-al, ay, fma(ga, s.wy, ly)));
+        lz = fma(c, s.tz, fma(-al, az, fma(ga, s.wz, lz)));
 
         ax = bx; ay = by; az = bz;
-        la = lb; ila = ilb;
-        hax = hbx; hay = hby; haz = hbz;
-        ca = cb;
-        qx = ey * hbz - ez * hby; qy = ez * hbx - ex * hbz; qz = ex * hby - ey * hbx;
-        if ((k & 63) == 63) {                                   // keep |z| near 1
+        la2 = lb2; la = lb; ila = ilb;
+        ea = eb;
+        if ((k & 15) == 15) {                                           // keep |z| in range
             const double sc = rcp_nr(fabs(zr) + fabs(zi));
             zr *= sc; zi *= sc;
         }
@@ -131,25 +150,30 @@ __device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, doub
 // Field at P (an atom moved by minus an image shift) of one line piece.
 // Follows Code/barnett.hpp:55-106 term by term (see field.cu's header for the
 // reformulations); adds b Omega/(4 pi) + the line terms to (ux, uy, uz).
-// For every segment, RA + RB >= 2 (l1 - rho) with l1 = |apex - P| and rho the
-// piece's largest vertex radius, so t = L/(RA+RB) <= lmax / (2 (l1 - rho)).
+// Vertices are stored relative to the apex; r = apex - P.  For every segment,
+// RA + RB >= 2 (l1 - rho) with l1 = |apex - P| and rho the piece's largest
+// vertex radius, so t = L/(RA+RB) <= lmax / (2 (l1 - rho)).
 __device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineSeg* seg,
                                                 double Px, double Py, double Pz, double cJ, double cK,
                                                 double& ux, double& uy, double& uz)
 {
     // unit vector from P to the fan apex
-    const double r1x = pc.cx - Px, r1y = pc.cy - Py, r1z = pc.cz - Pz;
-    const double l1sq = r1x * r1x + r1y * r1y + r1z * r1z;
-    const double il1 = rsqrt(l1sq);
-    const double ex = r1x * il1, ey = r1y * il1, ez = r1z * il1;
+    const double rx = pc.cx - Px, ry = pc.cy - Py, rz = pc.cz - Pz;
+    const double l1sq = rx * rx + ry * ry + rz * rz;
+    const double il1 = rsqrt_nr(l1sq);
+    const double ex = rx * il1, ey = ry * il1, ez = rz * il1;
     const double gap = l1sq * il1 - pc.rho;
-    const bool far_lane = gap > 0.0 && pc.lmax <= 2.0 * kSeriesTau * gap;
-    const bool far = __all_sync(__activemask(), far_lane);
+    const unsigned mine = gap > 0.0 ? series_tier(pc.lmax, 2.0 * gap) : 0u;
+    const unsigned tier = __reduce_min_sync(__activemask(), mine);
 
     double zr = 1.0, zi = 0.0, lx = 0.0, ly = 0.0, lz = 0.0;
-    const double ax = pc.ax - Px, ay = pc.ay - Py, az = pc.az - Pz;
-    if (far) line_segments<true>(seg, pc.nseg, Px, Py, Pz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz);
-    else     line_segments<false>(seg, pc.nseg, Px, Py, Pz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz);
+    const double ax = pc.ax + rx, ay = pc.ay + ry, az = pc.az + rz;
+    switch (tier) {
+    case 3:  line_segments<4>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz); break;
+    case 2:  line_segments<6>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz); break;
+    case 1:  line_segments<8>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz); break;
+    default: line_segments<0>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz); break;
+    }
     const double f = atan2(zi, zr) * (1.0 / 6.283185307179586476925286766559);   // Omega / (4 pi)
     ux += pc.bx * f + lx;
     uy += pc.by * f + ly;
@@ -344,12 +368,13 @@ inline void make_line_piece(const disco_loop& lp, int k0, int k1e, double bx, do
     const int nv = lp.n_vertices;
     std::memset(&p, 0, sizeof(p));
     const int a = (k0 + nv - 1) % nv;
-    p.ax = lp.vx[a]; p.ay = lp.vy[a]; p.az = lp.vz[a];
-    p.cx = lp.cx; p.cy = lp.cy; p.cz = lp.cz;
+    const double c[3] = { lp.cx, lp.cy, lp.cz };
+    p.ax = lp.vx[a] - c[0]; p.ay = lp.vy[a] - c[1]; p.az = lp.vz[a] - c[2];
+    p.cx = c[0]; p.cy = c[1]; p.cz = c[2];
     p.bx = bx; p.by = by; p.bz = bz;
     p.nseg = k1e - k0;
     auto radius = [&](int k) {
-        const double dx = lp.vx[k] - lp.cx, dy = lp.vy[k] - lp.cy, dz = lp.vz[k] - lp.cz;
+        const double dx = lp.vx[k] - c[0], dy = lp.vy[k] - c[1], dz = lp.vz[k] - c[2];
         return std::sqrt(dx * dx + dy * dy + dz * dz);
     };
     p.rho = radius(a);
@@ -358,7 +383,11 @@ inline void make_line_piece(const disco_loop& lp, int k0, int k1e, double bx, do
         const int km = (k + nv - 1) % nv;
         LineSeg s;
         std::memset(&s, 0, sizeof(s));
-        s.vx = lp.vx[k]; s.vy = lp.vy[k]; s.vz = lp.vz[k];
+        s.vx = lp.vx[k] - c[0]; s.vy = lp.vy[k] - c[1]; s.vz = lp.vz[k] - c[2];
+        const double ux = lp.vx[km] - c[0], uy = lp.vy[km] - c[1], uz = lp.vz[km] - c[2];
+        s.nx = uy * s.vz - uz * s.vy;
+        s.ny = uz * s.vx - ux * s.vz;
+        s.nz = ux * s.vy - uy * s.vx;
         const double tx = lp.vx[k] - lp.vx[km], ty = lp.vy[k] - lp.vy[km], tz = lp.vz[k] - lp.vz[km];
         const double L = std::sqrt(tx * tx + ty * ty + tz * tz);
         if (L > 0.0) {

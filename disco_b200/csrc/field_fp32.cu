@@ -91,10 +91,11 @@ int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, H
                     s64.push_back(sg);
                     LineSegF f;
                     std::memset(&f, 0, sizeof(f));
-                    f.vx = (float)(sg.vx - c[0]); f.vy = (float)(sg.vy - c[1]); f.vz = (float)(sg.vz - c[2]);
+                    f.vx = (float)sg.vx; f.vy = (float)sg.vy; f.vz = (float)sg.vz;     // apex-relative
                     f.len = (float)sg.len;
                     f.tx = (float)sg.tx; f.ty = (float)sg.ty; f.tz = (float)sg.tz;
                     f.wx = (float)sg.wx; f.wy = (float)sg.wy; f.wz = (float)sg.wz;
+                    f.nx = (float)sg.nx; f.ny = (float)sg.ny; f.nz = (float)sg.nz;
                     recs.push_back(f);
                 }
                 p64.push_back(q);

@@ -41,7 +41,11 @@ struct AccF32K {
 };
 
 // Code/barnett.hpp:44-107 in FP32 on centre-relative coordinates, with the
-// same reformulation as line_piece_fp64.
+// same reformulation as line_piece_fp64: the solid angle as the argument of
+// the product of unnormalised Van Oosterom-Strackee factors (renormalised
+// every 4 segments, well inside the FP32 range), e.(a x b) from the segment's
+// precomputed (A - apex) x (B - apex), cK folded into d.w.  d = a - sA t is
+// formed explicitly here (in FP32, |a|^2 - sA^2 would cancel).
 __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const LineSegF* seg, float Px,
                                                 float Py, float Pz, float cJ, float cK,
                                                 float& ux, float& uy, float& uz)
@@ -53,9 +57,7 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
     float la2 = ax * ax + ay * ay + az * az;
     float ila = rsqrtf(la2);
     float la = la2 * ila;
-    float hax = ax * ila, hay = ay * ila, haz = az * ila;
-    float ca = ex * hax + ey * hay + ez * haz;
-    float qx = ey * haz - ez * hay, qy = ez * hax - ex * haz, qz = ex * hay - ey * hax;
+    float ea = ex * ax + ey * ay + ez * az;
     float zr = 1.0f, zi = 0.0f, lx = 0.0f, ly = 0.0f, lz = 0.0f;
     const int nseg = pc.nseg;
     for (int k = 0; k < nseg; ++k) {
@@ -64,10 +66,9 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
         const float lb2 = bx * bx + by * by + bz * bz;
         const float ilb = rsqrtf(lb2);
         const float lb = lb2 * ilb;
-        const float hbx = bx * ilb, hby = by * ilb, hbz = bz * ilb;
-        const float cb = ex * hbx + ey * hby + ez * hbz;
-        const float den = 1.0f + ca + cb + (hax * hbx + hay * hby + haz * hbz);
-        const float num = qx * hbx + qy * hby + qz * hbz;
+        const float eb = ex * bx + ey * by + ez * bz;
+        const float den = fmaf(ea, lb, fmaf(eb, la, fmaf(la, lb, ax * bx + ay * by + az * bz)));
+        const float num = ex * s.nx + ey * s.ny + ez * s.nz;
         const float nzr = zr * den - zi * num;
         zi = zr * num + zi * den;
         zr = nzr;
@@ -75,22 +76,19 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
         const float sB = sA + s.len;
         const float dx = ax - sA * s.tx, dy = ay - sA * s.ty, dz = az - sA * s.tz;
         const float d2 = dx * dx + dy * dy + dz * dz;
-        const float dw = dx * s.wx + dy * s.wy + dz * s.wz;
+        const float dw = cK * (dx * s.wx + dy * s.wy + dz * s.wz);
         const float sum = la + lb;
-        const float J0 = __logf(__fdividef(sum + s.len, sum - s.len));
+        const float ga = cJ * __logf(__fdividef(sum + s.len, sum - s.len));
         const float g = sB * ilb - sA * ila;
-        const float q = d2 > 0.0f ? __fdividef(dw, d2) : 0.0f;
-        const float K1 = ila - ilb;
-        const float al = cK * q * g, be = cK * dw * K1, ga = cJ * J0;
+        const float al = d2 > 0.0f ? __fdividef(dw, d2) * g : 0.0f;
+        const float be = dw * (ila - ilb);
         lx += ga * s.wx - al * dx - be * s.tx;
         ly += ga * s.wy - al * dy - be * s.ty;
         lz += ga * s.wz - al * dz - be * s.tz;
         ax = bx; ay = by; az = bz;
         la = lb; ila = ilb;
-        hax = hbx; hay = hby; haz = hbz;
-        ca = cb;
-        qx = ey * hbz - ez * hby; qy = ez * hbx - ex * hbz; qz = ex * hby - ey * hbx;
-        if ((k & 15) == 15) {
+        ea = eb;
+        if ((k & 3) == 3) {
             const float sc = __frcp_rn(fabsf(zr) + fabsf(zi));
             zr *= sc; zi *= sc;
         }

@@ -310,6 +310,15 @@ int disco_b200_learned_displace(disco_mlp *m, const disco_far_norm *norm, const 
                                 const disco_learned_options *opt, disco_learned_report *report,
                                 void *stream);
 
+/* ---- self-test ---------------------------------------------------------------------- */
+
+/* Evaluates one of the kernels' own FP64 routines on DEVICE arrays, so that
+ * tests can hold them against CUDA's functions: fn 0: 1/sqrt(x) (hardware
+ * approximation + one Householder step), 1: 1/x (approximation + one cubic
+ * Newton-Raphson step), 2, 3, 4: 2 atanh(x) by the 8-, 6- and 4-term series
+ * of the far-field J0.  No counterpart in the reference. */
+int disco_b200_math_check(int32_t fn, const double *x, double *y, int64_t n, void *stream);
+
 /* ---- prismatic loops: slab selection and stream compaction ------------------------ */
 
 /* One loop of the matter step.  Geometry as in the reference's loop class

@@ -208,13 +208,16 @@ def cpu_baseline(w, seconds, use_reference):
             u = O.displace(x, y, z, w.loops, w.box, images=w.images, nu=w.nu, threads=threads)
         return time.perf_counter() - t0, u
 
-    k = max(threads, 8)
-    idx = np.sort(rng.choice(w.n, size=min(k, w.n), replace=False))
-    dt, _ = run(idx)
-    rate = len(idx) / dt
-    k = int(min(w.n, max(len(idx), rate * seconds)))
+    # calibrate: a small probe, then samples scaled to the target time (at most 3 runs)
+    k = min(w.n, 4 * threads)
     idx = np.sort(rng.choice(w.n, size=k, replace=False))
     dt, u = run(idx)
+    for _ in range(3):
+        if dt >= 0.5 * seconds or k >= w.n:
+            break
+        k = int(min(w.n, max(2 * k, k * seconds / max(dt, 1e-3))))
+        idx = np.sort(rng.choice(w.n, size=k, replace=False))
+        dt, u = run(idx)
     kind = "reference" if ref_ok else "port"
     what = ("the reference's kroupaCPU compiled from its sources (oracle/_ref), nu fixed at 0.35 "
             "in the reference, same operation count") if ref_ok else \
@@ -235,28 +238,32 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     ref_ok = w.images == 1 and O.have_ref()
     rng = np.random.default_rng(99)
-    # bounded sample per step so that warmup + steps stay within a few minutes
-    probe = np.sort(rng.choice(w.n, size=max(threads, 8), replace=False))
-    t0 = time.perf_counter()
-    if ref_ok:
-        O.ref_displace(w.x[probe], w.y[probe], w.z[probe], w.loops, w.box)
-    else:
-        O.displace(w.x[probe], w.y[probe], w.z[probe], w.loops, w.box, images=w.images, nu=w.nu,
-                   threads=threads)
-    rate = len(probe) / (time.perf_counter() - t0)
-    per_step = max(8.0, min(25.0, 150.0 / max(1, args.steps + args.warmup)))
-    k = int(min(w.n, max(len(probe), rate * per_step)))
-    times = []
-    for s in range(args.warmup + args.steps):
-        idx = np.sort(rng.choice(w.n, size=k, replace=False))
+
+    def run(idx):
         t0 = time.perf_counter()
         if ref_ok:
             O.ref_displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box)
         else:
             O.displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box, images=w.images, nu=w.nu,
                        threads=threads)
+        return time.perf_counter() - t0
+
+    # bounded sample per step so that warmup + steps stay within a few minutes:
+    # a small probe, then samples scaled to the per-step target (at most 3 runs)
+    per_step = max(8.0, min(25.0, 150.0 / max(1, args.steps + args.warmup)))
+    k = min(w.n, 4 * threads)
+    dt = run(np.sort(rng.choice(w.n, size=k, replace=False)))
+    for _ in range(3):
+        if dt >= 0.25 * per_step or k >= w.n:
+            break
+        k = int(min(w.n, max(2 * k, 0.5 * k * per_step / max(dt, 1e-3))))
+        dt = run(np.sort(rng.choice(w.n, size=k, replace=False)))
+    k = int(min(w.n, max(k, k * per_step / max(dt, 1e-3))))
+    times = []
+    for s in range(args.warmup + args.steps):
+        dt = run(np.sort(rng.choice(w.n, size=k, replace=False)))
         if s >= args.warmup:
-            times.append(time.perf_counter() - t0)
+            times.append(dt)
     T = sum(times)
     value = k * args.steps / T
     kind = "reference" if ref_ok else "port"

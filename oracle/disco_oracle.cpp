@@ -207,6 +207,11 @@ int oracle_displace_shells(const disco_atoms* atoms, const disco_loop* loops, in
     const double k1 = 1.0 / (8.0 * M_PI * (1.0 - nu));
     const double c2 = 1.0 - 2.0*nu;
     const int I = images;
+    // The reference's chunk of 256 atoms; smaller on samples too small to give
+    // every thread a chunk (scheduling only: the arithmetic per atom is fixed).
+    const int nthr = omp_get_max_threads();
+    const int chunk = nbAtoms >= (int64_t)256 * 4 * nthr ? 256
+                    : (int)std::max<int64_t>(1, nbAtoms / (4 * (int64_t)nthr));
     for (int l = 0; l < nloops; l++) {
         const disco_loop& lp = loops[l];
         const double t0 = omp_get_wtime();
@@ -214,7 +219,7 @@ int oracle_displace_shells(const disco_atoms* atoms, const disco_loop* loops, in
             const int nv = lp.n_vertices;
             const double bx = lp.phys.bx * lp.phys.mx, by = lp.phys.by * lp.phys.my,
                          bz = lp.phys.bz * lp.phys.mz;
-#pragma omp parallel for schedule(dynamic, 256)
+#pragma omp parallel for schedule(dynamic, chunk)
             for (int64_t a = 0; a < nbAtoms; a++) {
                 double dux = 0., duy = 0., duz = 0.;
                 for (int ii = -I; ii <= I; ii++)
@@ -235,7 +240,7 @@ int oracle_displace_shells(const disco_atoms* atoms, const disco_loop* loops, in
             const double* ly = lp.y;
             const double* lz = lp.z;
             const double b_n = L.mx*L.nx + L.my*L.ny + L.mz*L.nz;
-#pragma omp parallel for schedule(dynamic, 256)
+#pragma omp parallel for schedule(dynamic, chunk)
             for (int64_t a = 0; a < nbAtoms; a++) {
                 const double ax = atoms->x[a], ay = atoms->y[a], az = atoms->z[a];
                 double dux = 0., duy = 0., duz = 0.;

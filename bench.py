@@ -71,6 +71,18 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(value, world, device="cuda"):
+    """The largest of the ranks' values (every rank gets it); value itself when
+    world == 1.  Timings of a multi-GPU run are the slowest rank's."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def build_workload(name, images=None):
     from disco_b200 import workloads as W
     w = W.FULL[name]()
@@ -324,10 +336,7 @@ def run_ours(args):
     clk = clocks.stop()
     plan.sync(stream.cuda_stream)
     elapsed = e0.elapsed_time(e1) * 1e-3
-    if world > 1:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(elapsed, world)
     per_launch = elapsed / args.steps
     value = n * world * args.steps / elapsed
 
@@ -354,10 +363,7 @@ def run_ours(args):
                      images=w.images, nu=w.nu, image_split=args.image_split)
     barrier()
     e2e_t = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_t], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks(e2e_t, world)
     e2e = {"value": n * world * e2e_steps / e2e_t, "unit": "atoms/s",
            "h2d_bytes_per_step": 6 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n, "steps": e2e_steps}
 
@@ -449,10 +455,7 @@ def run_batch(args):
     clk = clocks.stop()
     plan.sync(stream.cuda_stream)
     elapsed = e0.elapsed_time(e1) * 1e-3
-    if world > 1:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(elapsed, world)
     per = elapsed / args.steps
     # parity: a fresh sum on a few samples against the oracle
     for q in u:
@@ -507,6 +510,13 @@ def run_batch(args):
         e2e = {"value": n * world / e2e_t, "unit": "atoms/s", "h2d_bytes_per_step": 48 * n,
                "d2h_bytes_per_step": 24 * n, "steps": 1}
     if rank == 0:
+        peak = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else fp32_peak_tflops(torch)
+        achieved = evals * W_LINE / per / 1e12
+        roof = {"bound": "fp32" if prec != C.DISCO_FP64 else "fp64", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "flop_per_eval": W_LINE,
+                "evals_per_launch": evals,
+                "peak_source": "measured here: torch " + ("DGEMM" if prec == C.DISCO_FP64 else
+                                                          "SGEMM without TF32") + " 8192^3, best of 5"}
         line = {
             "metric": METRIC, "value": n * world / per, "unit": "atoms/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per,
@@ -521,9 +531,7 @@ def run_batch(args):
                        "l2": f"inputs larger than L2 ({24 * n / 1e9:.2f} GB of positions)",
                        "parallelism": f"replicas x{world}"},
             "evals_per_s": evals * world / per,
-            "roofline": {"bound": "fp32" if prec != C.DISCO_FP64 else "fp64",
-                         "achieved": evals * W_LINE / per / 1e12, "peak": None, "unit": "TFLOP/s",
-                         "frac": None, "traffic": None},
+            "roofline": roof,
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": args.steps * (2 if prec == C.DISCO_FP32C else 1), "parity": parity,
         }
@@ -585,10 +593,7 @@ def run_learned(args):
     barrier()
     clk = clocks.stop()
     elapsed = e0.elapsed_time(e1) * 1e-3
-    if world > 1:
-        t = torch.tensor([elapsed], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(elapsed, world)
     per = elapsed / args.steps
 
     # accuracy on every atom against the plain FP64 path (+-4, all images exact)
@@ -635,10 +640,7 @@ def run_learned(args):
         hp[3:].copy_(du_, non_blocking=True)
         torch.cuda.synchronize()
     e2e_t = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_t], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks(e2e_t, world)
     e2e = {"value": n * world * e2e_steps / e2e_t, "unit": "atoms/s", "h2d_bytes_per_step": 48 * n,
            "d2h_bytes_per_step": 24 * n, "steps": e2e_steps}
     if rank == 0:
@@ -683,6 +685,160 @@ def run_learned(args):
         dist.destroy_process_group()
 
 
+def run_prismatic(args):
+    """Config 3: one step = the prismatic matter step (slab selection, vacancy
+    removal, interstitial copies; disco_b200_prismatic_noalloc on device
+    arrays), the loopon field of all 16 loops over the surviving atoms (plan),
+    and the fused copy/add-u/wrap epilogue (disco_b200_finalize_resident).
+    value = input atoms / step time.  Parity: atom sets, order, copies bit-exact
+    against the oracle; the field on a seeded survivor sample within 1e-9 A
+    (FP64); the final positions of that sample against the oracle's epilogue."""
+    import ctypes
+    import torch
+    from disco_b200 import backend as B
+    from disco_b200 import _capi as C
+    from disco_b200 import prismatic as P
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    lib = C.cuda_lib()
+    w = build_workload("bcc_prismatic", args.images)
+    prec = C.DISCO_FP32C if args.precision == "fp32c" else C.DISCO_FP64
+    n = w.n
+    first = P.prismatic(w.x, w.y, w.z, w.slab_loops, w.box)       # capacities for the device arrays
+    ns0, nc0 = len(first["slab_atoms"]), len(first["copy_atom"])
+    scap, ccap = ns0 + 1024, nc0 + 1024
+    plan = B.Plan(w.loops, w.box, precision=prec, images=w.images, nu=w.nu, image_split=args.image_split,
+                  max_atoms=n)
+    st_plan = plan.stats()
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
+    out = torch.empty((3, n), dtype=torch.float64, device="cuda")
+    new_index = torch.empty(n, dtype=torch.int32, device="cuda")
+    slab_atoms = torch.empty(scap, dtype=torch.int32, device="cuda")
+    slab_side = torch.empty(scap, dtype=torch.int8, device="cuda")
+    copies = torch.empty((ccap, 4), dtype=torch.float64, device="cuda")
+    u = torch.zeros((3, n), dtype=torch.float64, device="cuda")
+    fin = torch.empty((6, n + ccap), dtype=torch.float64, device="cuda")
+    nl = len(w.slab_loops)
+    sl = (C.DiscoSlabLoop * nl)(*w.slab_loops)
+    info = (C.DiscoSlabInfo * nl)()
+    counts = (ctypes.c_int64 * 3)()
+    box = (ctypes.c_double * 3)(*w.box)
+
+    def step():
+        C.check(lib.disco_b200_prismatic_noalloc(
+            pos[0].data_ptr(), pos[1].data_ptr(), pos[2].data_ptr(), n, sl, nl, box,
+            out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), new_index.data_ptr(), info,
+            slab_atoms.data_ptr(), slab_side.data_ptr(), scap, copies.data_ptr(), ccap, counts, sp), lib)
+        k, nc = int(counts[0]), int(counts[2])
+        u[:, :k].zero_()
+        plan.execute_ptrs(out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), u[0].data_ptr(),
+                          u[1].data_ptr(), u[2].data_ptr(), k, stream.cuda_stream)
+        tot = k + nc
+        C.check(lib.disco_b200_finalize_resident(
+            out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), u[0].data_ptr(), u[1].data_ptr(),
+            u[2].data_ptr(), k, copies.data_ptr(), nc, box, fin[0].data_ptr(), fin[1].data_ptr(),
+            fin[2].data_ptr(), fin[3].data_ptr(), fin[4].data_ptr(), fin[5].data_ptr(), sp), lib)
+        return k, nc
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    plan.sync(stream.cuda_stream)
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        k, nc = step()
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    plan.sync(stream.cuda_stream)
+    elapsed = e0.elapsed_time(e1) * 1e-3
+    elapsed = max_over_ranks(elapsed, world)
+    per = elapsed / args.steps
+    evals = st_plan["evals_per_atom"] * k
+
+    # e2e: the host entry points (matter step, kroupa_gpu drop-in, epilogue) on host arrays
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else 2
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        r = P.prismatic(w.x, w.y, w.z, w.slab_loops, w.box)
+        sx, sy, sz = r["survivors"]
+        atoms = B.AtomArrays.zeros_like_positions(sx, sy, sz)
+        B.kroupa_gpu(atoms, w.loops, *w.box, B.GpuOptions(fp32=prec == C.DISCO_FP32C), images=w.images,
+                     nu=w.nu)
+        final = P.finalize(sx, sy, sz, atoms.ux, atoms.uy, atoms.uz, r["copy_atom"], r["copy_shift"], w.box)
+    e2e_t = max_over_ranks(time.perf_counter() - t0, world)
+
+    parity = None
+    cpu = None
+    if rank == 0:
+        import oracle as O
+        ref = O.prismatic(w.x, w.y, w.z, w.slab_loops, w.box)
+        o = out.cpu().numpy()
+        sets = (int(counts[0]) == len(ref["survivors"][0]) and
+                all(np.array_equal(o[d, :k], ref["survivors"][d]) for d in range(3)) and
+                np.array_equal(new_index.cpu().numpy(), ref["new_index"]) and
+                np.array_equal(slab_atoms.cpu().numpy()[:int(counts[1])], ref["slab_atoms"]) and
+                np.array_equal(copies.cpu().numpy()[:nc, 1:], ref["copy_shift"]))
+        rng = np.random.default_rng(5)
+        idx = np.sort(rng.choice(k, size=min(k, 2000), replace=False))
+        ug = u.cpu().numpy()[:, idx]
+        uo = np.stack(O.displace(o[0, idx], o[1, idx], o[2, idx], w.loops, w.box, images=w.images, nu=w.nu))
+        f = fin.cpu().numpy()[:3, idx]
+        fo = np.stack(O.finalize(o[0, idx], o[1, idx], o[2, idx], ug[0], ug[1], ug[2],
+                                 np.zeros(0, np.int32), np.zeros((0, 3)), w.box)[:3])
+        parity = {"atom_sets_bit_exact": bool(sets), "max_abs_du": float(np.abs(ug - uo).max()),
+                  "final_positions_bit_exact_on_sample": bool(np.array_equal(f, fo)),
+                  "atoms": int(len(idx)), "survivors": k, "copies": nc, "against": "oracle"}
+        if not args.no_cpu:
+            cpu, _, _ = cpu_baseline(w, args.cpu_seconds, use_reference=False)
+            cpu.pop("seconds", None)
+            cpu["sample"] += "; the matter step is not in the CPU figure (host serial in the reference, ms)"
+        peak = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else fp32_peak_tflops(torch)
+        achieved = evals * W_LOOPON / per / 1e12
+        line = {
+            "metric": METRIC, "value": n * world / per, "unit": "atoms/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if prec == C.DISCO_FP64 else "f32c", "data": "synthetic",
+            "config": {"workload": "bcc_prismatic", "atoms": n, "survivors": k, "copies": nc,
+                       "loops": len(w.loops), "loopons": st_plan["n_loopons"], "images": st_plan["n_images"],
+                       "nu": w.nu, "method": "loopons", "precision": args.precision,
+                       "step": "matter step + loopon field + copy/add-u/wrap epilogue, all on device",
+                       "l2": "inputs fit in L2 (10 MB of positions); no flush (compute-bound: the "
+                             "field is >99 % of the step)", "parallelism": f"replicas x{world}"},
+            "evals_per_s": evals * world / per,
+            "roofline": {"bound": "fp64" if prec == C.DISCO_FP64 else "fp32", "kernel": "loopon field",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "traffic": None, "flop_per_eval": W_LOOPON, "evals_per_launch": evals},
+            "cpu_baseline": cpu,
+            "e2e": {"value": n * world * e2e_steps / e2e_t, "unit": "atoms/s",
+                    "h2d_bytes_per_step": 24 * n + 48 * k + 48 * k,
+                    "d2h_bytes_per_step": 28 * n + 24 * k + 48 * (k + nc), "steps": e2e_steps},
+            "clocks": clk, "gpu_launches": args.steps * 6,     # count, scan, scatter, copies, field, epilogue
+            "parity": parity,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def ctypes_byref(x):
     import ctypes
     return ctypes.byref(x)
@@ -698,6 +854,8 @@ def main():
         run_batch(args)
     elif args.config == "learned":
         run_learned(args)
+    elif args.config == "bcc_prismatic":
+        run_prismatic(args)
     else:
         run_ours(args)
 

@@ -200,6 +200,8 @@ def cuda_lib():
              [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64,
               POINTER(DiscoCopy), c_int64, POINTER(c_double), c_void_p, c_void_p, c_void_p,
               c_void_p, c_void_p, c_void_p])
+        _sig(lib, "disco_b200_finalize_resident", c_int,
+             [c_void_p] * 6 + [c_int64, c_void_p, c_int64, POINTER(c_double)] + [c_void_p] * 7)
         _cuda = lib
     return _cuda
 

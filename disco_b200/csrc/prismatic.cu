@@ -639,6 +639,27 @@ int disco_b200_finalize(const double* x, const double* y, const double* z,
     return DISCO_OK;
 }
 
+int disco_b200_finalize_resident(const double* x, const double* y, const double* z,
+                                 const double* ux, const double* uy, const double* uz, int64_t n,
+                                 const disco_copy* copies, int64_t ncopies, const double box[3],
+                                 double* fx, double* fy, double* fz,
+                                 double* ux_out, double* uy_out, double* uz_out, void* stream)
+{
+    if (n < 0 || ncopies < 0 || !box || (n > 0 && (!x || !y || !z || !ux || !uy || !uz)) ||
+        (ncopies > 0 && (!copies || n == 0)) || (n + ncopies > 0 && (!fx || !fy || !fz)))
+        return efail(DISCO_EINVAL, "null or negative argument");
+    const bool want_u = ux_out && uy_out && uz_out;
+    const int64_t tot = n + ncopies;
+    if (tot == 0) return DISCO_OK;
+    const int threads = 256;
+    const int64_t blocks = std::min<int64_t>((tot + threads - 1) / threads, 148 * 16);
+    disco::finalize_kernel<<<(unsigned)blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(
+        x, y, z, ux, uy, uz, n, copies, ncopies, box[0], box[1], box[2], fx, fy, fz,
+        want_u ? ux_out : nullptr, uy_out, uz_out);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? DISCO_OK : cfail(e, "finalize launch");
+}
+
 } // extern "C"
 
 // ---- matter step without allocation ---------------------------------------------------

@@ -415,6 +415,16 @@ int disco_b200_finalize(const double *x, const double *y, const double *z,
                         double *fx, double *fy, double *fz,
                         double *ux_out, double *uy_out, double *uz_out);
 
+/* Resident form of disco_b200_finalize: every array, copies included, is a
+ * DEVICE pointer (copies as written by disco_b200_prismatic_noalloc); the
+ * kernel runs on `stream` and the call returns without waiting.  Copy sources
+ * must lie in [0, n) (they do when they come from the matter step). */
+int disco_b200_finalize_resident(const double *x, const double *y, const double *z,
+                                 const double *ux, const double *uy, const double *uz, int64_t n,
+                                 const disco_copy *copies, int64_t ncopies, const double box[3],
+                                 double *fx, double *fy, double *fz,
+                                 double *ux_out, double *uy_out, double *uz_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,7 @@ def parse():
     p.add_argument("--retrain", action="store_true", help="learned: train the network even if cached")
     p.add_argument("--epochs", type=int, default=32, help="learned: training epochs over 2^22 samples")
     p.add_argument("--no-fp64", action="store_true", help="learned: skip the plain FP64 comparison run")
+    p.add_argument("--no-output", action="store_true", help="skip the output-writer measurement")
     return p.parse_args()
 
 
@@ -294,6 +295,63 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+ELEMENTS = {("fcc", 3.615): "Cu", ("bcc", 2.855): "Fe", ("bcc", 3.165): "W"}
+
+
+def write_output(w, pos, u, stream):
+    """The output epilogue after the field, outside the timed step: final
+    positions (disco_b200_finalize_resident: add u, wrap, shift) and the XYZ
+    atom lines (disco_b200_format_atoms) on the device, then the text to
+    pinned host memory; checked byte for byte against the oracle's stream
+    formatting on the first 200 000 atoms, and the oracle's formatting rate on
+    one host thread (the reference writes with one ofstream) for comparison."""
+    import ctypes
+    import torch
+    import oracle as O
+    from disco_b200 import _capi as C
+    from disco_b200 import geometry as G
+    lib = C.cuda_lib()
+    n = pos.shape[1]
+    elem = ELEMENTS.get(("fcc" if w.lattice == G.FCC else "bcc", round(w.a0, 3)), "X")
+    fin = torch.empty((3, n), dtype=torch.float64, device="cuda")
+    cap = 72 * n + 64
+    text = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    host = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+    box = (ctypes.c_double * 3)(*w.box)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    nbytes = ctypes.c_int64()
+
+    def once():
+        C.check(lib.disco_b200_finalize_resident(pos[0].data_ptr(), pos[1].data_ptr(), pos[2].data_ptr(),
+                                                 u[0].data_ptr(), u[1].data_ptr(), u[2].data_ptr(), n, None, 0,
+                                                 box, fin[0].data_ptr(), fin[1].data_ptr(), fin[2].data_ptr(),
+                                                 None, None, None, sp), lib)
+        C.check(lib.disco_b200_format_atoms(0, elem.encode(), fin[0].data_ptr(), fin[1].data_ptr(),
+                                            fin[2].data_ptr(), n, text.data_ptr(), cap, ctypes.byref(nbytes), sp),
+                lib)
+        host[:nbytes.value].copy_(text[:nbytes.value], non_blocking=True)
+
+    once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    once()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    m = min(n, 200000)
+    f = fin[:, :m].cpu().numpy()
+    t1 = time.perf_counter()
+    ref = O.format_atoms(0, elem, f[0], f[1], f[2])
+    cpu_rate = m / (time.perf_counter() - t1)
+    ok = bytes(host[:len(ref)].numpy()) == ref
+    return {"what": "finalize + XYZ atom lines on the device + text to pinned host memory",
+            "atoms": n, "bytes": int(nbytes.value), "ms": e0.elapsed_time(e1), "wall_ms": 1e3 * wall,
+            "atoms_per_s": n / (e0.elapsed_time(e1) * 1e-3), "bytes_match_oracle_first_atoms": m if ok else 0,
+            "cpu_oracle_atoms_per_s_1_thread": cpu_rate}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -341,10 +399,12 @@ def run_ours(args):
     value = n * world * args.steps / elapsed
 
     # parity on a seeded sample (fresh sum) while the CPU baseline runs on it
-    u1 = torch.zeros_like(pos)
-    plan.execute(pos, u1)
+    u1d = torch.zeros_like(pos)
+    plan.execute(pos, u1d)
     plan.sync(stream.cuda_stream)
-    u1 = u1.cpu().numpy()
+    u1 = u1d.cpu().numpy()
+    output = write_output(w, pos, u1d, stream) if (rank == 0 and not args.no_output) else None
+    del u1d
 
     # e2e: the public host call on pinned host memory
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
@@ -399,7 +459,7 @@ def run_ours(args):
                        f"{24 * n / 1e6:.0f} MB)", "parallelism": f"replicas x{world}"},
             "evals_per_s": evals_atom * n * world * args.steps / elapsed,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": launches_per_step * args.steps, "parity": parity,
+            "gpu_launches": launches_per_step * args.steps, "parity": parity, "output": output,
         }
         print(json.dumps(line), flush=True)
     plan.close()

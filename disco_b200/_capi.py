@@ -178,6 +178,11 @@ def cuda_lib():
              [c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
               c_void_p])
         _sig(lib, "disco_b200_mlp_status", c_int, [c_void_p])
+        _sig(lib, "disco_b200_format_atoms", c_int,
+             [c_int32, c_char_p, c_void_p, c_void_p, c_void_p, c_int64, c_void_p, c_int64, POINTER(c_int64),
+              c_void_p])
+        _sig(lib, "disco_b200_lattice", c_int,
+             [c_int32, c_int32, c_int32, c_int32, c_double, c_void_p, c_void_p, c_void_p, c_void_p])
         _sig(lib, "disco_b200_math_check", c_int, [c_int32, c_void_p, c_void_p, c_int64, c_void_p])
         _sig(lib, "disco_b200_far_features", c_int,
              [POINTER(DiscoAtoms), POINTER(DiscoLoop), c_int32, POINTER(c_double), POINTER(DiscoFarNorm),

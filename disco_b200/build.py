@@ -23,7 +23,7 @@ NVCC = os.environ.get("DISCO_NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("DISCO_CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CUDA_SOURCES = ["field.cu", "field_fp32.cu", "batch.cu", "mlp.cu", "far.cu", "prismatic.cu", "capi.cu"]
+CUDA_SOURCES = ["field.cu", "field_fp32.cu", "batch.cu", "mlp.cu", "far.cu", "prismatic.cu", "lattice.cu", "writer.cu", "capi.cu"]
 CUDA_HEADERS = ["common.cuh", "field.cuh", "field_device.cuh", "field_fp32.cuh", "tcgen05.cuh", "mlp.cuh"]
 
 LIB_CUDA = os.path.join(LIB, "libdisco_b200.so")

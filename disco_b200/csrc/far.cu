@@ -218,8 +218,10 @@ __global__ void __launch_bounds__(kFarThreads, 2) far_kernel(const FarArgs a)
         const int64_t ia = valid ? atom : a.n - 1;
         const double px = a.x[ia], py = a.y[ia], pz = a.z[ia];
         float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+        FarLoop L = a.loops[a.sel[0]];
         for (int s = 0; s < a.nsel; ++s) {
-            const FarLoop& L = a.loops[a.sel[s]];
+            // the next loop's descriptor loads while this loop's layers run
+            const FarLoop next = a.loops[a.sel[s + 1 < a.nsel ? s + 1 : s]];
             {
                 float f[16];
                 features(px, py, pz, L, a.fn, f);
@@ -256,6 +258,7 @@ __global__ void __launch_bounds__(kFarThreads, 2) far_kernel(const FarArgs a)
                 sy += gy;
                 sz += gz;
             }
+            L = next;
         }
         if (ok && valid && !a.per_loop) {
             a.ux[atom] += sx;

@@ -310,6 +310,33 @@ int disco_b200_learned_displace(disco_mlp *m, const disco_far_norm *norm, const 
                                 const disco_learned_options *opt, disco_learned_report *report,
                                 void *stream);
 
+/* ---- input on the device ------------------------------------------------------------ */
+
+/* Perfect-lattice sites written straight into DEVICE arrays x, y, z of
+ * 2 (BCC, lattice 0) or 4 (FCC, lattice 1) x nx x ny x nz entries:
+ * Code/lattice.hpp:35-51 (generateLattice), same order, bit-identical
+ * positions, without the host build and the host-to-device copy.  Runs on
+ * `stream` and returns without waiting. */
+int disco_b200_lattice(int32_t lattice, int32_t nx, int32_t ny, int32_t nz, double a0,
+                       double *x, double *y, double *z, void *stream);
+
+/* ---- output ------------------------------------------------------------------------- */
+
+/* The atom lines of the output files, formatted on the device as the
+ * reference's C++ streams format them (`fixed << setprecision(8)`: exact
+ * decimal rounding, ties to even).  format 0: XYZ, "<element> x y z\n"
+ * (Code/main.cpp:826-831); format 1: LAMMPS atomic, "<k+1> 1 x y z\n"
+ * (Code/main.cpp:86-92) for an orthorhombic box, whose projection onto the
+ * LAMMPS frame is the identity.  x, y, z: DEVICE arrays of final positions
+ * (e.g. from disco_b200_finalize_resident), |v| < 1.8e11; out: DEVICE buffer of
+ * `capacity` bytes; *bytes = the text's length.  A short buffer returns
+ * DISCO_ELIMIT with *bytes = the size needed.  The call waits for the line
+ * lengths, then launches the writing kernel on `stream` and returns.  The
+ * header lines stay with the caller (they hold a handful of numbers). */
+int disco_b200_format_atoms(int32_t format, const char *element, const double *x, const double *y,
+                            const double *z, int64_t n, char *out, int64_t capacity, int64_t *bytes,
+                            void *stream);
+
 /* ---- self-test ---------------------------------------------------------------------- */
 
 /* Evaluates one of the kernels' own FP64 routines on DEVICE arrays, so that

@@ -78,6 +78,9 @@ def _load(path):
             lib.oracle_displace_shells.argtypes = [POINTER(C.DiscoAtoms), POINTER(C.DiscoLoop), c_int,
                                                    POINTER(c_double), c_int, c_int, c_double, c_int,
                                                    c_void_p]
+            lib.oracle_format_atoms.restype = c_int64
+            lib.oracle_format_atoms.argtypes = [c_int, ctypes.c_char_p, c_void_p, c_void_p, c_void_p, c_int64,
+                                                c_void_p, c_int64]
             lib.oracle_prismatic.restype = c_int
             lib.oracle_prismatic.argtypes = [c_void_p, c_void_p, c_void_p, c_int64,
                                              POINTER(C.DiscoSlabLoop), c_int32, POINTER(c_double),
@@ -227,6 +230,18 @@ def slab_margins(x, y, z, slab_loops, box):
     lib.oracle_slab_margins(x.ctypes.data, y.ctypes.data, z.ctypes.data, len(x), arr, nl, _box(box),
                             out.ctypes.data)
     return out
+
+
+def format_atoms(fmt, element, x, y, z):
+    """oracle_format_atoms: the writers' atom lines as bytes (0 XYZ, 1 LAMMPS)."""
+    lib = oracle_lib(False)
+    x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+    n = len(x)
+    need = lib.oracle_format_atoms(fmt, element.encode(), x.ctypes.data, y.ctypes.data, z.ctypes.data, n, None, 0)
+    buf = ctypes.create_string_buffer(max(1, need))
+    lib.oracle_format_atoms(fmt, element.encode(), x.ctypes.data, y.ctypes.data, z.ctypes.data, n,
+                            ctypes.addressof(buf), need)
+    return buf.raw[:need]
 
 
 def finalize(x, y, z, ux, uy, uz, copy_atom, copy_shift, box):

@@ -24,6 +24,9 @@
 #include <cstdlib>
 #include <cstdint>
 #include <cstring>
+#include <iomanip>
+#include <sstream>
+#include <string>
 #include <vector>
 #include <omp.h>
 
@@ -446,3 +449,28 @@ int oracle_slab_margins(const double* x, const double* y, const double* z, int64
 }
 
 } // extern "C"
+
+// The atom lines of the reference's writers, through the same C++ stream
+// formatting: XYZ (format 0, Code/main.cpp:826-831) and LAMMPS atomic
+// (format 1, Code/main.cpp:86-92, with e1, e2, e3 the unit axes of an
+// orthorhombic box).  Returns the byte count; writes at most cap bytes.
+extern "C" int64_t oracle_format_atoms(int format, const char* element, const double* x, const double* y, const double* z,
+                            int64_t n, char* out, int64_t cap)
+{
+    std::ostringstream os;
+    os << std::fixed << std::setprecision(8);
+    const double e1[3] = { 1., 0., 0. }, e2[3] = { 0., 1., 0. }, e3[3] = { 0., 0., 1. };
+    for (int64_t k = 0; k < n; k++) {
+        if (format == 0) {
+            os << element << " " << x[k] << " " << y[k] << " " << z[k] << "\n";
+        } else {
+            os << k+1 << " 1 "
+               << e1[0]*x[k] + e1[1]*y[k] + e1[2]*z[k] << " "
+               << e2[0]*x[k] + e2[1]*y[k] + e2[2]*z[k] << " "
+               << e3[0]*x[k] + e3[1]*y[k] + e3[2]*z[k] << "\n";
+        }
+    }
+    const std::string s = os.str();
+    if ((int64_t)s.size() <= cap && out) std::memcpy(out, s.data(), s.size());
+    return (int64_t)s.size();
+}

@@ -3,7 +3,8 @@ same GPU): 1/sqrt(x) and 1/x within 1 ulp of CUDA's correctly rounded results
 (the displacement kernels then stay within 1e-9 A of the oracle, which the
 parity tests check end to end); the far-field series of 2 atanh(t) within
 3 ulps (6.7e-16 relative) of CUDA's atanh, itself within 2 ulps, over each
-tier's range."""
+tier's range.  Also the device lattice builder, bit-identical to the host
+restatement of generateLattice."""
 import ctypes
 
 import numpy as np
@@ -55,3 +56,16 @@ def test_series_matches_atanh(fn, tmax):
     ref = 2.0 * torch.atanh(x)
     rel = ((y - ref).abs() / ref.abs().clamp_min(1e-300)).max().item()
     assert rel <= 3 * 2.0 ** -52
+
+
+@pytest.mark.parametrize("kind,a0,cells", [(1, 3.615, (37, 38, 39)), (0, 2.855, (40, 41, 42)),
+                                           (0, 3.165, (60, 60, 60))])
+def test_device_lattice_is_bit_identical_to_the_host_build(kind, a0, cells):
+    from disco_b200 import geometry as G
+    lib = C.cuda_lib()
+    x, y, z = G.lattice(kind, *cells, a0)
+    d = torch.full((3, len(x)), float("nan"), dtype=torch.float64, device="cuda")
+    C.check(lib.disco_b200_lattice(kind, *cells, a0, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                   ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)), lib)
+    got = d.cpu().numpy()
+    assert np.array_equal(got[0], x) and np.array_equal(got[1], y) and np.array_equal(got[2], z)

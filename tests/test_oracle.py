@@ -327,3 +327,20 @@ def test_prismatic_pins_on_config_geometry():
         t = s / spacing
         assert np.all((t >= -1) & (t < 2))
         assert np.array_equal(r["slab_side"][off:off + cnt], np.where(s > 0, 1, -1))
+
+
+def test_oracle_writer_lines_match_correctly_rounded_formatting():
+    """The oracle's writer lines (the reference's C++ stream formatting) equal
+    Python's correctly rounded '%.8f' on the same doubles, ties included."""
+    rng = np.random.default_rng(3)
+    v = np.concatenate([rng.uniform(-600, 600, 3000), np.arange(1, 4001, 2) / 512.0,
+                        np.array([0.0, -0.0, -1e-12, 1e-9, 5e-9, 2.5e-8, 123456789.123456789])])
+    v = v[: (len(v) // 3) * 3]
+    x, y, z = v[0::3], v[1::3], v[2::3]
+    got = O.format_atoms(0, "Fe", x, y, z).decode()
+    want = "".join(f"Fe {a:.8f} {b:.8f} {c:.8f}\n" for a, b, c in zip(x, y, z))
+    assert got == want
+    got = O.format_atoms(1, "Fe", np.abs(x), np.abs(y), np.abs(z)).decode()
+    want = "".join(f"{k + 1} 1 {a:.8f} {b:.8f} {c:.8f}\n"
+                   for k, (a, b, c) in enumerate(zip(np.abs(x), np.abs(y), np.abs(z))))
+    assert got == want

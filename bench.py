@@ -492,7 +492,7 @@ def run_batch(args):
     ptrs = [(p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr(), q[0].data_ptr(), q[1].data_ptr(),
              q[2].data_ptr()) for p, q in zip(pos, u)]
     plan = B.BatchPlan(batch, ptrs, precision=prec, image_split=tune["image_split"],
-                       stage_kb=tune["stage_kb"])
+                       stage_kb=tune["stage_kb"], stages=tune["stages"])
     stream = torch.cuda.current_stream()
 
     def barrier():
@@ -561,6 +561,7 @@ def run_batch(args):
             arr[i].atoms = C.DiscoAtoms(*(hv[k].ctypes.data for k in range(6)), batch[i].n)
         o = B.options(prec, 1, batch[0].nu, tune["image_split"])
         o.stage_kb = tune["stage_kb"]
+        o.stages = tune["stages"]
         tm = C.DiscoTiming(0.0, 0.0, 0.0, None)
         barrier()
         t0 = time.perf_counter()
@@ -586,7 +587,8 @@ def run_batch(args):
                        "loops": sum(len(w.loops) for w in batch), "evals_per_step": evals,
                        "images": "+-1..+-3 per sample", "nu": batch[0].nu,
                        "precision": "fp64" if prec == C.DISCO_FP64 else "fp32c",
-                       "tuning": {"image_split": tune["image_split"], "stage_kb": tune["stage_kb"]},
+                       "tuning": {"image_split": tune["image_split"], "stage_kb": tune["stage_kb"],
+                                  "stages": tune["stages"]},
                        "graph": "one CUDA graph replay per step",
                        "l2": f"inputs larger than L2 ({24 * n / 1e9:.2f} GB of positions)",
                        "parallelism": f"replicas x{world}"},

@@ -48,7 +48,7 @@ class DiscoOptions(Structure):
                 ("chunk_pairs", c_double), ("atoms_per_thread", c_int32),
                 ("threads_per_block", c_int32), ("image_split", c_int32), ("verbose", c_int32),
                 ("near_plane", c_double), ("near_rim", c_double), ("stage_kb", c_int32),
-                ("image_min", c_int32)]
+                ("image_min", c_int32), ("stages", c_int32), ("reserved", c_int32)]
 
 
 class DiscoSample(Structure):

@@ -261,7 +261,7 @@ def sample_array(workloads, us=None, device_ptrs=None):
     return arr, keep
 
 
-def batch_gpu(workloads, precision=C.DISCO_FP64, nu=None, image_split=0, stage_kb=0):
+def batch_gpu(workloads, precision=C.DISCO_FP64, nu=None, image_split=0, stage_kb=0, stages=0):
     """The batched form on host arrays: returns [(ux, uy, uz)] per sample."""
     lib = C.cuda_lib()
     nu = workloads[0].nu if nu is None else nu
@@ -269,6 +269,7 @@ def batch_gpu(workloads, precision=C.DISCO_FP64, nu=None, image_split=0, stage_k
     arr, keep = sample_array(workloads, us)
     o = options(precision, 1, nu, image_split)
     o.stage_kb = stage_kb
+    o.stages = stages
     tm = C.DiscoTiming(0.0, 0.0, 0.0, None)
     C.check(lib.disco_b200_batch(arr, len(workloads), ctypes.byref(o), ctypes.byref(tm)), lib)
     del keep
@@ -280,12 +281,13 @@ class BatchPlan:
     atoms are device arrays given as [(x, y, z, ux, uy, uz) pointers]."""
 
     def __init__(self, workloads, device_ptrs, *, precision=C.DISCO_FP64, nu=None, image_split=0,
-                 stage_kb=0):
+                 stage_kb=0, stages=0):
         self._lib = C.cuda_lib()
         nu = workloads[0].nu if nu is None else nu
         arr, keep = sample_array(workloads, device_ptrs=device_ptrs)
         o = options(precision, 1, nu, image_split)
         o.stage_kb = stage_kb
+        o.stages = stages
         h = ctypes.c_void_p()
         C.check(self._lib.disco_b200_batch_plan_create(arr, len(workloads), ctypes.byref(o),
                                                        ctypes.byref(h)), self._lib)

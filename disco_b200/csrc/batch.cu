@@ -43,11 +43,14 @@ struct UnitDev {
     int32_t pad;
 };
 
+constexpr int kMaxStages = 4;
+
 struct BatchArgs {
     const SampleDev* samples;
     const UnitDev* units;
     const int32_t* cta_first;       // units of CTA b: [cta_first[b], cta_first[b + 1])
     uint32_t stage_bytes;
+    int32_t stages;                 // table stages in flight (2..kMaxStages)
     double cJ, cK, c2;
     float near_h, near_r;
     int* status;
@@ -65,9 +68,9 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
     const int u0 = b.cta_first[blockIdx.x];
     const int nunits = b.cta_first[blockIdx.x + 1] - u0;
     if (nunits <= 0) return;
+    const int D = b.stages;
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int j = 0; j < D; ++j) mbar_init(&bar[j], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -75,12 +78,10 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
         const UnitDev un = b.units[u0 + u];
         const SampleDev& sd = b.samples[un.sample];
         const Chunk c = sd.chunks[un.chunk];
-        stage_load(stage0 + (size_t)(u & 1) * b.stage_bytes, sd.table + c.offset, c.bytes, &bar[u & 1]);
+        stage_load(stage0 + (size_t)(u % D) * b.stage_bytes, sd.table + c.offset, c.bytes, &bar[u % D]);
     };
-    if (tid == 0) {
-        issue(0);
-        if (nunits > 1) issue(1);
-    }
+    if (tid == 0)
+        for (int j = 0; j < D && j < nunits; ++j) issue(j);
     constexpr int kAtomsPerTile = kBatchThreads / S;
     const int split = tid % S;
     double px = 0.0, py = 0.0, pz = 0.0;
@@ -98,14 +99,14 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
             px = sd.x[ia]; py = sd.y[ia]; pz = sd.z[ia];
             acc.clear();
         }
-        const int buf = u & 1;
-        const uint32_t parity = (uint32_t)((u >> 1) & 1);
+        const int buf = u % D;
+        const uint32_t parity = (uint32_t)((u / D) & 1);
         const bool ok = mbar_wait_bounded(&bar[buf], parity);
         if (__syncthreads_or(!ok)) {
+            // give up: record it, let every copy still in flight land (bounded), return
             if (tid == 0) {
                 report(b.status, DISCO_ETIMEOUT);
-                mbar_wait_bounded(&bar[buf], parity);
-                if (u + 1 < nunits) mbar_wait_bounded(&bar[buf ^ 1], (uint32_t)(((u + 1) >> 1) & 1));
+                for (int j = u; j < u + D && j < nunits; ++j) mbar_wait_bounded(&bar[j % D], (uint32_t)((j / D) & 1));
             }
             __syncthreads();
             return;
@@ -135,9 +136,9 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
             }
         }
         __syncthreads();                           // every warp is done with stage[buf]
-        if (tid == 0 && u + 2 < nunits) {
+        if (tid == 0 && u + D < nunits) {
             fence_proxy_async_smem();
-            issue(u + 2);
+            issue(u + D);
         }
     }
 }
@@ -151,6 +152,7 @@ struct disco_batch_plan {
     disco_options opt;
     int nsamples = 0;
     int split = 1;
+    int stages = 2;
     uint32_t stage_bytes = 0;
     // per kind (0 line, 1 loopon)
     unsigned char* d_table[2] = { nullptr, nullptr };
@@ -199,7 +201,7 @@ template <class Policy>
 int launch_batch_policy(const disco::BatchArgs& a, int grid, int split, cudaStream_t s, std::string& err)
 {
     using namespace disco;
-    const size_t smem = kSmemHeader + 2 * (size_t)a.stage_bytes;
+    const size_t smem = kSmemHeader + (size_t)a.stages * a.stage_bytes;
     void (*kern)(BatchArgs) = nullptr;
     switch (split) {
     case 1: kern = batch_kernel<Policy, 1>; break;
@@ -213,6 +215,34 @@ int launch_batch_policy(const disco::BatchArgs& a, int grid, int split, cudaStre
     e = cudaGetLastError();
     if (e != cudaSuccess) { err = cudaGetErrorString(e); return DISCO_ECUDA; }
     return DISCO_OK;
+}
+
+// Resident CTAs per SM of the batch kernel(s) of one loop kind at `smem` bytes.
+template <class Policy>
+int occupancy_of(int split, size_t smem)
+{
+    using namespace disco;
+    void (*kern)(BatchArgs) = nullptr;
+    switch (split) {
+    case 1: kern = batch_kernel<Policy, 1>; break;
+    case 2: kern = batch_kernel<Policy, 2>; break;
+    case 4: kern = batch_kernel<Policy, 4>; break;
+    default: kern = batch_kernel<Policy, 8>; break;
+    }
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchThreads, smem) != cudaSuccess)
+        return 0;
+    return per_sm;
+}
+
+int occupancy(int kind, bool fp32, int split, size_t smem)
+{
+    using namespace disco;
+    if (kind == kLineKind)
+        return fp32 ? std::min(occupancy_of<LineFp32>(split, smem), occupancy_of<LineNearFp64>(split, smem))
+                    : occupancy_of<LineFp64>(split, smem);
+    return fp32 ? occupancy_of<LooponFp32>(split, smem) : occupancy_of<LooponFp64>(split, smem);
 }
 
 // Launches every kernel of the plan on stream s (used once, under capture).
@@ -229,6 +259,7 @@ int launch_all(disco_batch_plan* p, cudaStream_t s)
         a.units = p->d_units[k];
         a.cta_first = p->d_cta_first[k];
         a.stage_bytes = p->stage_bytes;
+        a.stages = p->stages;
         a.cJ = c3 - 1.0 / (4.0 * pi);
         a.cK = c3;
         a.c2 = 1.0 - 2.0 * p->opt.nu;
@@ -270,6 +301,10 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
         return bfail(DISCO_EINVAL, "batched image_split must be 1, 2, 4 or 8");
     const uint32_t stage = (uint32_t)(o.stage_kb > 0 ? o.stage_kb : 48) * 1024u;
     if (stage < 16 * 1024u || stage > 100 * 1024u) return bfail(DISCO_EINVAL, "stage_kb must be in 16..100");
+    const int stages = o.stages > 0 ? o.stages : 2;
+    if (stages < 2 || stages > kMaxStages) return bfail(DISCO_EINVAL, "stages must be in 2..4");
+    if (kSmemHeader + (size_t)stages * stage > 227u * 1024u)
+        return bfail(DISCO_EINVAL, "stages x stage_kb exceeds the 227 KB of shared memory of a CTA");
     for (int s = 0; s < nsamples; ++s) {
         const disco_sample& sm = samples[s];
         if (sm.images < 0 || sm.images > 8) return bfail(DISCO_EINVAL, "sample images must be in 0..8");
@@ -285,6 +320,7 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
     p->opt = o;
     p->nsamples = nsamples;
     p->split = split;
+    p->stages = stages;
     p->fp32 = o.precision == DISCO_FP32C;
     std::memset(&p->stats, 0, sizeof(p->stats));
     cudaError_t e = cudaGetDevice(&p->device);
@@ -293,7 +329,6 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
     if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(int));
     if (e != cudaSuccess) { free_batch(p); return bcuda(e, "device setup"); }
     const int atoms_per_tile = kBatchThreads / split;
-    const int grid_max = p->sm_count * 2;
     uint32_t max_stage = 16;
     double evals = 0.0;
     for (int k = 0; k < 2; ++k) {
@@ -377,6 +412,10 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
             }
         }
         std::stable_sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.cost > b.cost; });
+        // as many CTAs as fit on the GPU at once, so that the greedy balance holds
+        const int per_sm = occupancy(kind, p->fp32, split, kSmemHeader + (size_t)stages * stage);
+        if (per_sm < 1) { free_batch(p); return bfail(DISCO_ECUDA, "batch kernel does not fit on an SM"); }
+        const int grid_max = p->sm_count * per_sm;
         const int grid = (int)std::min<size_t>(std::max<size_t>(items.size(), 1), (size_t)grid_max);
         std::vector<std::vector<int>> per_cta(grid);
         using Load = std::pair<double, int>;

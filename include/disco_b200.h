@@ -113,6 +113,9 @@ typedef struct {
                                   0 = automatic (resident up to 110 KB, else 48)  */
     int32_t image_min;         /* skip the images with max(|i|,|j|,|k|) < image_min:
                                   2 sums only the far shells 2 <= max|n| <= images */
+    int32_t stages;            /* batched form: table stages in flight per CTA (the
+                                  copy pipeline's depth), 2..4; 0 = 2             */
+    int32_t reserved;
 } disco_options;
 
 /* Phase timings, seconds: Code/backend.hpp:36-39 (BackendTiming).

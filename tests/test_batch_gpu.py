@@ -69,3 +69,24 @@ def test_batch_plan_graph_replay_accumulates():
         assert np.abs(q.cpu().numpy() - 2 * ref).max() <= 2e-9
     st = plan.stats()
     assert st["evals_per_atom"] == sum(w.n * w.evals_per_atom() for w in batch)
+
+
+@pytest.mark.parametrize("stages,stage_kb", [(3, 16), (4, 24), (3, 48)])
+def test_batch_pipeline_depths(stages, stage_kb):
+    """Deeper copy pipelines (3 and 4 stages in flight) give the same sums."""
+    batch = _small_batch(seed=14, n=5)
+    big = W.batch(nsamples=1, edge=(6, 6), nloops=(10, 10), radius=(8.0, 9.0), segments=(120, 128),
+                  images=(1, 1), seed=15)[0]
+    allw = batch + [big]
+    us, _ = B.batch_gpu(allw, C.DISCO_FP64, stage_kb=stage_kb, stages=stages)
+    for w, u in zip(allw, us):
+        ref = O.displace(w.x, w.y, w.z, w.loops, w.box, images=w.images, nu=w.nu)
+        assert max(np.abs(u[k] - ref[k]).max() for k in range(3)) <= 1e-9, w.name
+
+
+def test_batch_rejects_bad_depth():
+    batch = _small_batch(seed=16, n=2)
+    with pytest.raises(C.DiscoError):
+        B.batch_gpu(batch, C.DISCO_FP64, stages=5)
+    with pytest.raises(C.DiscoError):
+        B.batch_gpu(batch, C.DISCO_FP64, stage_kb=100, stages=3)

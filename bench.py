@@ -72,6 +72,16 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", 0))
 
 
+def measured_peaks():
+    """The pool's measured peaks (HBM copy GB/s, BF16 TFLOP/s) from
+    MEASURED_PEAKS.json beside this file, or None."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return json.load(open(path))
+    except (OSError, ValueError):
+        return None
+
+
 def max_over_ranks(value, world, device="cuda"):
     """The largest of the ranks' values (every rank gets it); value itself when
     world == 1.  Timings of a multi-GPU run are the slowest rank's."""
@@ -747,6 +757,57 @@ def run_learned(args):
         dist.destroy_process_group()
 
 
+def compaction_rate(lib, C, torch, stream):
+    """The matter step alone (disco_b200_prismatic_noalloc: slab membership,
+    stable compaction, new-index map, copies) on the largest box it takes,
+    BCC 128^3 = 4 194 304 atoms with 16 loops of the bcc_prismatic distribution:
+    achieved GB/s of the algorithmic bytes (76 B per atom: positions read twice,
+    survivors written, 4 B index) against the measured HBM peak.  The call
+    includes two small device-to-host reads of the counts (its host syncs)."""
+    import ctypes
+    from disco_b200 import workloads as W
+    w = W.bcc_prismatic(cells=128)
+    n = w.n
+    pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
+    out = torch.empty((3, n), dtype=torch.float64, device="cuda")
+    new_index = torch.empty(n, dtype=torch.int32, device="cuda")
+    cap = 1 << 21
+    slab_atoms = torch.empty(cap, dtype=torch.int32, device="cuda")
+    slab_side = torch.empty(cap, dtype=torch.int8, device="cuda")
+    copies = torch.empty((cap, 4), dtype=torch.float64, device="cuda")
+    nl = len(w.slab_loops)
+    sl = (C.DiscoSlabLoop * nl)(*w.slab_loops)
+    info = (C.DiscoSlabInfo * nl)()
+    counts = (ctypes.c_int64 * 3)()
+    box = (ctypes.c_double * 3)(*w.box)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def call():
+        C.check(lib.disco_b200_prismatic_noalloc(
+            pos[0].data_ptr(), pos[1].data_ptr(), pos[2].data_ptr(), n, sl, nl, box,
+            out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), new_index.data_ptr(), info,
+            slab_atoms.data_ptr(), slab_side.data_ptr(), cap, copies.data_ptr(), cap, counts, sp), lib)
+
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    reps = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / reps
+    pk = measured_peaks()
+    peak = pk["hbm_gbs"] if pk else 6650.0
+    gbs = 76.0 * n / t / 1e9
+    return {"atoms": n, "survivors": int(counts[0]), "slab_atoms": int(counts[1]), "copies": int(counts[2]),
+            "ms": 1e3 * t, "atoms_per_s": n / t, "algorithmic_bytes": 76 * n, "achieved_gbs": gbs,
+            "peak_gbs": peak, "frac": gbs / peak,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk else "fallback 6650 GB/s"}
+
+
 def run_prismatic(args):
     """Config 3: one step = the prismatic matter step (slab selection, vacancy
     removal, interstitial copies; disco_b200_prismatic_noalloc on device
@@ -845,6 +906,7 @@ def run_prismatic(args):
         final = P.finalize(sx, sy, sz, atoms.ux, atoms.uy, atoms.uz, r["copy_atom"], r["copy_shift"], w.box)
     e2e_t = max_over_ranks(time.perf_counter() - t0, world)
 
+    compaction = compaction_rate(lib, C, torch, stream) if rank == 0 else None
     parity = None
     cpu = None
     if rank == 0:
@@ -892,7 +954,7 @@ def run_prismatic(args):
                     "h2d_bytes_per_step": 24 * n + 48 * k + 48 * k,
                     "d2h_bytes_per_step": 28 * n + 24 * k + 48 * (k + nc), "steps": e2e_steps},
             "clocks": clk, "gpu_launches": args.steps * 6,     # count, scan, scatter, copies, field, epilogue
-            "parity": parity,
+            "parity": parity, "compaction": compaction,
         }
         print(json.dumps(line), flush=True)
     plan.close()

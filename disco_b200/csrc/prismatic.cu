@@ -41,6 +41,8 @@ struct SlabLoopDev {
     disco_slab_loop L;
     double tLo, tHi;       // slab bounds in units of d (Code/prismatic.cpp:58-59)
     double cuv, det;       // u.v and 1 - (u.v)^2 (Code/loop.cpp:327-328)
+    float nf[3], cf[3];    // the pre-test only: n, c, 1 / spacing, its margin in planes
+    float inv_df, margin;
     int32_t type;          // DISCO_MATTER_VACANCY or DISCO_MATTER_INTERSTITIAL
     int32_t pad;
 };
@@ -92,6 +94,33 @@ __device__ bool inside_uv_rn(const disco_slab_loop& g, double u, double v)
     return __dadd_rn(__dmul_rn(du, du), __dmul_rn(dv, dv)) <= __dadd_rn(__dmul_rn(g.r_corner, g.r_corner), eps);
 }
 
+// Cheap pre-test in FP32: true only if the atom's t is outside [tLo, tHi) by
+// more than `margin` planes.  With the atom and the centre rounded to FP32
+// and the nearest image unambiguous (r/L + 1/2 at least 1e-5 from an integer
+// and |r/L| < 2, else it returns false), the FP32 t differs from the exactly
+// rounded t of slab_member by less than 1.5e-6 (Lx + Ly + Lz) / d + 1e-6
+// planes; the margin is 1e-5 (Lx + Ly + Lz) / d + 1e-3.  So it never rejects
+// a member: the exact test below decides every atom it passes, and atom sets
+// stay bit-exact.
+__device__ __forceinline__ bool clearly_outside(const SlabLoopDev& S, const float (&p)[3], const float (&L)[3],
+                                                const float (&iL)[3])
+{
+    float s = 0.0f;
+    bool sure = true;                     // branch-free, so that loops interleave
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float r = p[k] - S.cf[k];
+        const float q = r * iL[k];
+        const float h = q + 0.5f;
+        const float f = floorf(h);
+        const float fr = h - f;
+        sure = sure && fabsf(q) < 2.0f && fr >= 1e-5f && fr <= 1.0f - 1e-5f;
+        s = fmaf(S.nf[k], fmaf(-L[k], f, r), s);
+    }
+    const float t = s * S.inv_df;
+    return sure && (t < (float)S.tLo - S.margin || t >= (float)S.tHi + S.margin);
+}
+
 // Slab membership of one atom (Code/prismatic.cpp:61-72); side = sign of s.
 __device__ __forceinline__ bool slab_member(const SlabLoopDev& S, double x, double y, double z,
                                             double Lx, double Ly, double Lz, bool& pos_side)
@@ -118,6 +147,7 @@ struct SlabArgs {
     const SlabLoopDev* loops;
     int32_t nl;
     double Lx, Ly, Lz;
+    float iLx, iLy, iLz;      // 1 / box lengths in FP32 (the pre-test only)
     int32_t* tile_counts;     // [ntiles][nl + 1]
     int32_t* tile_offsets;    // [ntiles][nl + 1]
     int64_t* totals;          // [nl + 1] totals, [nl] loop bases, [1] copies
@@ -129,11 +159,22 @@ struct SlabArgs {
 
 // Every atom's membership mask over the active loops, sides and removal.
 __device__ __forceinline__ void atom_masks(const SlabLoopDev* sl, int nl, double x, double y, double z,
-                                           double Lx, double Ly, double Lz, uint64_t& mask,
-                                           uint64_t& sides, bool& removed)
+                                           const SlabArgs& a, uint64_t& mask, uint64_t& sides, bool& removed)
 {
+    const double Lx = a.Lx, Ly = a.Ly, Lz = a.Lz;
     mask = 0; sides = 0; removed = false;
-    for (int l = 0; l < nl; ++l) {
+    const float L[3] = { (float)Lx, (float)Ly, (float)Lz };
+    const float iL[3] = { a.iLx, a.iLy, a.iLz };
+    const float p[3] = { (float)x, (float)y, (float)z };
+    // the pre-test for every loop first (independent, interleaved), then the
+    // exact test for the loops it could not exclude, in loop order
+    uint64_t cand = 0;
+#pragma unroll 4
+    for (int l = 0; l < nl; ++l)
+        if (!clearly_outside(sl[l], p, L, iL)) cand |= 1ull << l;
+    while (cand) {
+        const int l = __ffsll((long long)cand) - 1;
+        cand &= cand - 1;
         bool ps = false;
         if (slab_member(sl[l], x, y, z, Lx, Ly, Lz, ps)) {
             mask |= 1ull << l;
@@ -151,6 +192,7 @@ __device__ __forceinline__ void load_loops(SlabLoopDev* dst, const SlabLoopDev* 
     for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = s[i];
 }
 
+// CTA b takes tiles b, b + grid, ... (with the grid of slab_grid: tile b).
 __global__ void __launch_bounds__(kSlabThreads) slab_count_kernel(const SlabArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -158,69 +200,83 @@ __global__ void __launch_bounds__(kSlabThreads) slab_count_kernel(const SlabArgs
     __shared__ int cnt[kMaxSlabLoops + 1];
     const int C = a.nl + 1;
     load_loops(sl, a.loops, a.nl);
-    for (int i = threadIdx.x; i < C; i += blockDim.x) cnt[i] = 0;
-    __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int64_t base = (int64_t)blockIdx.x * kSlabTile;
-    for (int r = 0; r < kSlabRounds; ++r) {
-        const int64_t i = base + r * kSlabThreads + threadIdx.x;
-        const bool valid = i < a.n;
-        uint64_t mask = 0, sides = 0;
-        bool removed = false;
-        if (valid) atom_masks(sl, a.nl, a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, mask, sides, removed);
-        const unsigned b0 = __ballot_sync(0xffffffffu, valid && !removed);
-        if (lane == 0 && b0) atomicAdd(&cnt[0], __popc(b0));
-        for (int l = 0; l < a.nl; ++l) {
-            const unsigned b = __ballot_sync(0xffffffffu, (mask >> l) & 1ull);
-            if (lane == 0 && b) atomicAdd(&cnt[1 + l], __popc(b));
+    const int64_t ntiles = (a.n + kSlabTile - 1) / kSlabTile;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        for (int i = threadIdx.x; i < C; i += blockDim.x) cnt[i] = 0;
+        __syncthreads();
+        const int64_t base = tile * kSlabTile;
+        for (int r = 0; r < kSlabRounds; ++r) {
+            const int64_t i = base + r * kSlabThreads + threadIdx.x;
+            const bool valid = i < a.n;
+            uint64_t mask = 0, sides = 0;
+            bool removed = false;
+            if (valid) atom_masks(sl, a.nl, a.x[i], a.y[i], a.z[i], a, mask, sides, removed);
+            const unsigned b0 = __ballot_sync(0xffffffffu, valid && !removed);
+            if (lane == 0 && b0) atomicAdd(&cnt[0], __popc(b0));
+            for (int l = 0; l < a.nl; ++l) {
+                const unsigned b = __ballot_sync(0xffffffffu, (mask >> l) & 1ull);
+                if (lane == 0 && b) atomicAdd(&cnt[1 + l], __popc(b));
+            }
         }
+        __syncthreads();
+        for (int c = threadIdx.x; c < C; c += blockDim.x)
+            a.tile_counts[tile * C + c] = cnt[c];
+        __syncthreads();
     }
-    __syncthreads();
-    for (int c = threadIdx.x; c < C; c += blockDim.x)
-        a.tile_counts[(int64_t)blockIdx.x * C + c] = cnt[c];
 }
 
-// One CTA: exclusive scan over tiles for every category; totals and bases.
+// One CTA per category (survivors, then each loop): exclusive scan over the
+// tiles, the category's total; the last CTA to finish (a counter in
+// totals[2 C], zeroed with the totals) writes the loops' bases.
 __global__ void __launch_bounds__(1024) slab_scan_kernel(const SlabArgs a, int64_t ntiles)
 {
     __shared__ int64_t warp_sum[32];
     __shared__ int64_t carry;
+    __shared__ bool last;
     const int C = a.nl + 1;
+    const int c = blockIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int c = 0; c < C; ++c) {
-        if (threadIdx.x == 0) carry = 0;
-        __syncthreads();
-        for (int64_t t0 = 0; t0 < ntiles; t0 += blockDim.x) {
-            const int64_t t = t0 + threadIdx.x;
-            const int64_t v = t < ntiles ? a.tile_counts[t * C + c] : 0;
-            int64_t x = v;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
-            }
-            if (lane == 31) warp_sum[warp] = x;
-            __syncthreads();
-            if (warp == 0) {
-                int64_t s = lane < (int)(blockDim.x >> 5) ? warp_sum[lane] : 0;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int64_t y = __shfl_up_sync(0xffffffffu, s, o);
-                    if (lane >= o) s += y;
-                }
-                warp_sum[lane] = s;           // inclusive over warps
-            }
-            __syncthreads();
-            const int64_t excl = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + x - v;
-            if (t < ntiles) a.tile_offsets[t * C + c] = (int32_t)excl;
-            __syncthreads();
-            if (threadIdx.x == 0) carry += warp_sum[(blockDim.x >> 5) - 1];
-            __syncthreads();
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int64_t t0 = 0; t0 < ntiles; t0 += blockDim.x) {
+        const int64_t t = t0 + threadIdx.x;
+        const int64_t v = t < ntiles ? a.tile_counts[t * C + c] : 0;
+        int64_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
         }
-        if (threadIdx.x == 0) a.totals[c] = carry;
+        if (lane == 31) warp_sum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int64_t s = lane < (int)(blockDim.x >> 5) ? warp_sum[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            warp_sum[lane] = s;           // inclusive over warps
+        }
+        __syncthreads();
+        const int64_t excl = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + x - v;
+        if (t < ntiles) a.tile_offsets[t * C + c] = (int32_t)excl;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += warp_sum[(blockDim.x >> 5) - 1];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
+        a.totals[c] = carry;
+        __threadfence();
+        const unsigned long long done =
+            atomicAdd(reinterpret_cast<unsigned long long*>(&a.totals[2 * C]), 1ull);
+        last = done == (unsigned long long)(C - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const volatile int64_t* tot = a.totals;
         int64_t acc = 0;
-        for (int l = 0; l < a.nl; ++l) { a.totals[C + l] = acc; acc += a.totals[1 + l]; }
+        for (int l = 0; l < a.nl; ++l) { a.totals[C + l] = acc; acc += tot[1 + l]; }
     }
 }
 
@@ -233,64 +289,67 @@ __global__ void __launch_bounds__(kSlabThreads) slab_scatter_kernel(const SlabAr
     __shared__ int64_t base_off[kMaxSlabLoops + 1];        // global offset of this tile per category
     const int C = a.nl + 1;
     load_loops(sl, a.loops, a.nl);
-    for (int c = threadIdx.x; c < C; c += blockDim.x) {
-        run[c] = 0;
-        const int64_t t = a.tile_offsets[(int64_t)blockIdx.x * C + c];
-        base_off[c] = c == 0 ? t : a.totals[C + (c - 1)] + t;
-    }
-    __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
-    const int64_t base = (int64_t)blockIdx.x * kSlabTile;
-    for (int r = 0; r < kSlabRounds; ++r) {
-        const int64_t i = base + r * kSlabThreads + threadIdx.x;
-        const bool valid = i < a.n;
-        uint64_t mask = 0, sides = 0;
-        bool removed = false;
-        double x = 0., y = 0., z = 0.;
-        if (valid) {
-            x = a.x[i]; y = a.y[i]; z = a.z[i];
-            atom_masks(sl, a.nl, x, y, z, a.Lx, a.Ly, a.Lz, mask, sides, removed);
-        }
-        const bool surv = valid && !removed;
-        const unsigned b0 = __ballot_sync(0xffffffffu, surv);
-        const int r0 = __popc(b0 & lt);
-        if (lane == 0) wcnt[warp][0] = __popc(b0);
-        for (int l = 0; l < a.nl; ++l) {
-            const unsigned b = __ballot_sync(0xffffffffu, (mask >> l) & 1ull);
-            if (lane == 0) wcnt[warp][1 + l] = __popc(b);
-        }
-        __syncthreads();
-        // exclusive prefix over the warps of this round, per category
+    const int64_t ntiles = (a.n + kSlabTile - 1) / kSlabTile;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         for (int c = threadIdx.x; c < C; c += blockDim.x) {
-            int acc = run[c];
-            for (int w = 0; w < kSlabWarps; ++w) {
-                const int v = wcnt[w][c];
-                wcnt[w][c] = acc;
-                acc += v;
-            }
-            run[c] = acc;
+            run[c] = 0;
+            const int64_t t = a.tile_offsets[tile * C + c];
+            base_off[c] = c == 0 ? t : a.totals[C + (c - 1)] + t;
         }
         __syncthreads();
-        if (valid) {
-            if (surv) {
-                const int64_t p = base_off[0] + wcnt[warp][0] + r0;
-                a.xo[p] = x; a.yo[p] = y; a.zo[p] = z;
-                a.new_index[i] = (int32_t)p;
-            } else {
-                a.new_index[i] = -1;
+        const int64_t base = tile * kSlabTile;
+        for (int r = 0; r < kSlabRounds; ++r) {
+            const int64_t i = base + r * kSlabThreads + threadIdx.x;
+            const bool valid = i < a.n;
+            uint64_t mask = 0, sides = 0;
+            bool removed = false;
+            double x = 0., y = 0., z = 0.;
+            if (valid) {
+                x = a.x[i]; y = a.y[i]; z = a.z[i];
+                atom_masks(sl, a.nl, x, y, z, a, mask, sides, removed);
             }
-        }
-        for (int l = 0; l < a.nl; ++l) {
-            const bool m = (mask >> l) & 1ull;
-            const unsigned b = __ballot_sync(0xffffffffu, m);
-            if (m) {
-                const int64_t p = base_off[1 + l] + wcnt[warp][1 + l] + __popc(b & lt);
-                a.slab_atoms[p] = (int32_t)i;
-                a.slab_side[p] = ((sides >> l) & 1ull) ? 1 : -1;
+            const bool surv = valid && !removed;
+            const unsigned b0 = __ballot_sync(0xffffffffu, surv);
+            const int r0 = __popc(b0 & lt);
+            if (lane == 0) wcnt[warp][0] = __popc(b0);
+            for (int l = 0; l < a.nl; ++l) {
+                const unsigned b = __ballot_sync(0xffffffffu, (mask >> l) & 1ull);
+                if (lane == 0) wcnt[warp][1 + l] = __popc(b);
             }
+            __syncthreads();
+            // exclusive prefix over the warps of this round, per category
+            for (int c = threadIdx.x; c < C; c += blockDim.x) {
+                int acc = run[c];
+                for (int w = 0; w < kSlabWarps; ++w) {
+                    const int v = wcnt[w][c];
+                    wcnt[w][c] = acc;
+                    acc += v;
+                }
+                run[c] = acc;
+            }
+            __syncthreads();
+            if (valid) {
+                if (surv) {
+                    const int64_t p = base_off[0] + wcnt[warp][0] + r0;
+                    a.xo[p] = x; a.yo[p] = y; a.zo[p] = z;
+                    a.new_index[i] = (int32_t)p;
+                } else {
+                    a.new_index[i] = -1;
+                }
+            }
+            for (int l = 0; l < a.nl; ++l) {
+                const bool m = (mask >> l) & 1ull;
+                const unsigned b = __ballot_sync(0xffffffffu, m);
+                if (m) {
+                    const int64_t p = base_off[1 + l] + wcnt[warp][1 + l] + __popc(b & lt);
+                    a.slab_atoms[p] = (int32_t)i;
+                    a.slab_side[p] = ((sides >> l) & 1ull) ? 1 : -1;
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
     }
 }
 
@@ -401,10 +460,18 @@ int efail(int code, const std::string& msg)
     return code;
 }
 
+// Grid of the tile kernels: one CTA per tile (a persistent grid of 4 CTAs
+// per SM measured 25 % slower: the per-round barriers of a tile want as many
+// CTAs in flight as the GPU holds).
+unsigned slab_grid(int64_t ntiles)
+{
+    return (unsigned)ntiles;
+}
+
 // One loop's SlabResult scalars (Code/prismatic.cpp:42-57) and, when it is
 // active (b.n != 0 and apply), its device record.  Never allocates.
-int slab_loop_record(const disco_slab_loop& g, int l, disco_slab_info& in, disco::SlabLoopDev& d,
-                     bool& active)
+int slab_loop_record(const disco_slab_loop& g, int l, const double box[3], disco_slab_info& in,
+                     disco::SlabLoopDev& d, bool& active)
 {
     std::memset(&in, 0, sizeof(in));
     active = false;
@@ -437,19 +504,25 @@ int slab_loop_record(const disco_slab_loop& g, int l, disco_slab_info& in, disco
     const double c = g.u[0] * g.v[0] + g.u[1] * g.v[1] + g.u[2] * g.v[2];
     d.cuv = c;
     d.det = 1.0 - c * c;
+    for (int k = 0; k < 3; ++k) {
+        d.nf[k] = (float)g.n[k];
+        d.cf[k] = (float)g.c[k];
+    }
+    d.inv_df = (float)(1.0 / in.spacing);
+    d.margin = (float)(1e-5 * (box[0] + box[1] + box[2]) / in.spacing + 1e-3);
     d.type = type;
     active = true;
     return DISCO_OK;
 }
 
 // Active loops in caller order.
-int prepare_loops(const disco_slab_loop* loops, int nloops, disco_slab_info* info,
+int prepare_loops(const disco_slab_loop* loops, int nloops, const double box[3], disco_slab_info* info,
                   std::vector<disco::SlabLoopDev>& act, std::vector<int>& act_index)
 {
     for (int l = 0; l < nloops; ++l) {
         disco::SlabLoopDev d;
         bool active = false;
-        const int st = slab_loop_record(loops[l], l, info[l], d, active);
+        const int st = slab_loop_record(loops[l], l, box, info[l], d, active);
         if (st) return st;
         if (!active) continue;
         if ((int)act.size() >= disco::kMaxSlabLoops) {
@@ -491,7 +564,7 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     if (cudaGetDeviceCount(&dcount) != cudaSuccess || dcount == 0) return efail(DISCO_ENODEV, "no CUDA device");
     std::vector<SlabLoopDev> act;
     std::vector<int> act_index;
-    int st = prepare_loops(loops, nloops, info, act, act_index);
+    int st = prepare_loops(loops, nloops, box, info, act, act_index);
     if (st) return st;
     const int nl = (int)act.size();
     const int C = nl + 1;
@@ -527,6 +600,7 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     a.loops = dloops.as<SlabLoopDev>();
     a.nl = nl;
     a.Lx = box[0]; a.Ly = box[1]; a.Lz = box[2];
+    a.iLx = (float)(1.0 / box[0]); a.iLy = (float)(1.0 / box[1]); a.iLz = (float)(1.0 / box[2]);
     a.tile_counts = dcnt.as<int32_t>();
     a.tile_offsets = doff.as<int32_t>();
     a.totals = dtot.as<int64_t>();
@@ -539,8 +613,8 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
             e = cudaFuncSetAttribute(slab_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return cfail(e, "prismatic smem");
     }
-    if (ntiles > 0) slab_count_kernel<<<(unsigned)ntiles, kSlabThreads, smem>>>(a);
-    slab_scan_kernel<<<1, 1024>>>(a, ntiles);
+    if (ntiles > 0) slab_count_kernel<<<slab_grid(ntiles), kSlabThreads, smem>>>(a);
+    slab_scan_kernel<<<(unsigned)C, 1024>>>(a, ntiles);
     std::vector<int64_t> tot(2 * C + 1, 0);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpy(tot.data(), dtot.p, tot.size() * sizeof(int64_t), cudaMemcpyDeviceToHost);
@@ -556,7 +630,7 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     if (e != cudaSuccess) return cfail(e, "prismatic slab buffers");
     a.slab_atoms = dslab.as<int32_t>();
     a.slab_side = dside.as<int8_t>();
-    if (ntiles > 0) slab_scatter_kernel<<<(unsigned)ntiles, kSlabThreads, smem>>>(a);
+    if (ntiles > 0) slab_scatter_kernel<<<slab_grid(ntiles), kSlabThreads, smem>>>(a);
     slab_copies_kernel<<<1, 1024>>>(a, dcop.as<disco_copy>(), inter_total);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpy(tot.data(), dtot.p, tot.size() * sizeof(int64_t), cudaMemcpyDeviceToHost);
@@ -749,7 +823,7 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     for (int l = 0; l < nloops; ++l) {
         SlabLoopDev d;
         bool active = false;
-        st = slab_loop_record(loops[l], l, info[l], d, active);
+        st = slab_loop_record(loops[l], l, box, info[l], d, active);
         if (st) return st;
         if (!active) continue;
         if (nl >= kMaxSlabLoops) return efail(DISCO_ELIMIT, "more than 64 prismatic loops in one call");
@@ -770,6 +844,7 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     a.loops = d_loops;
     a.nl = nl;
     a.Lx = box[0]; a.Ly = box[1]; a.Lz = box[2];
+    a.iLx = (float)(1.0 / box[0]); a.iLy = (float)(1.0 / box[1]); a.iLz = (float)(1.0 / box[2]);
     a.tile_counts = d_cnt;
     a.tile_offsets = d_off;
     a.totals = d_tot;
@@ -784,8 +859,8 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
             e = cudaFuncSetAttribute(slab_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return cfail(e, "prismatic smem");
     }
-    if (ntiles > 0) slab_count_kernel<<<(unsigned)ntiles, kSlabThreads, smem, s>>>(a);
-    slab_scan_kernel<<<1, 1024, 0, s>>>(a, ntiles);
+    if (ntiles > 0) slab_count_kernel<<<slab_grid(ntiles), kSlabThreads, smem, s>>>(a);
+    slab_scan_kernel<<<(unsigned)C, 1024, 0, s>>>(a, ntiles);
     int64_t tot[2 * (kMaxSlabLoops + 1) + 1];
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpyAsync(tot, d_tot, (size_t)(2 * C) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
@@ -812,7 +887,7 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     counts[2] = inter_total;         // upper bound until the copies pass has run
     if (slab_total > slab_capacity)
         return efail(DISCO_ELIMIT, "slab capacity too small (counts[1] holds the size needed)");
-    if (ntiles > 0) slab_scatter_kernel<<<(unsigned)ntiles, kSlabThreads, smem, s>>>(a);
+    if (ntiles > 0) slab_scatter_kernel<<<slab_grid(ntiles), kSlabThreads, smem, s>>>(a);
     slab_copies_kernel<<<1, 1024, 0, s>>>(a, copies, copy_capacity);
     e = cudaGetLastError();
     if (e == cudaSuccess)

@@ -72,3 +72,55 @@ def finalize(x, y, z, ux, uy, uz, copy_atom, copy_shift, box):
     C.check(lib.disco_b200_finalize(*[a.ctypes.data for a in arrs], n, cps, nc, _box(box),
                                     *[o.ctypes.data for o in out]), lib)
     return [o[:n + nc] for o in out]
+
+
+def _main():
+    """python -m disco_b200.prismatic [--cells N] [--reps R]: the matter step
+    (disco_b200_prismatic_noalloc) on device arrays, BCC N^3 cells with the 16
+    loops of the bcc_prismatic distribution, timed with CUDA events; the case
+    the compaction kernels' ncu summaries are taken on."""
+    import argparse
+    import torch
+    from . import workloads as W
+    p = argparse.ArgumentParser()
+    p.add_argument("--cells", type=int, default=128)
+    p.add_argument("--reps", type=int, default=5)
+    a = p.parse_args()
+    lib = C.cuda_lib()
+    w = W.bcc_prismatic(cells=a.cells)
+    n = w.n
+    pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
+    out = torch.empty((3, n), dtype=torch.float64, device="cuda")
+    new_index = torch.empty(n, dtype=torch.int32, device="cuda")
+    cap = 1 << 21
+    slab_atoms = torch.empty(cap, dtype=torch.int32, device="cuda")
+    slab_side = torch.empty(cap, dtype=torch.int8, device="cuda")
+    copies = torch.empty((cap, 4), dtype=torch.float64, device="cuda")
+    nl = len(w.slab_loops)
+    sl = (C.DiscoSlabLoop * nl)(*w.slab_loops)
+    info = (C.DiscoSlabInfo * nl)()
+    counts = (ctypes.c_int64 * 3)()
+    s = torch.cuda.current_stream()
+
+    def call():
+        C.check(lib.disco_b200_prismatic_noalloc(
+            pos[0].data_ptr(), pos[1].data_ptr(), pos[2].data_ptr(), n, sl, nl, _box(w.box),
+            out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), new_index.data_ptr(), info,
+            slab_atoms.data_ptr(), slab_side.data_ptr(), cap, copies.data_ptr(), cap, counts,
+            ctypes.c_void_p(s.cuda_stream)), lib)
+
+    call()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / a.reps
+    print(f"matter step: {n} atoms, {counts[0]} survivors, {counts[1]} slab atoms, {counts[2]} copies: "
+          f"{t * 1e3:.3f} ms per call, {76.0 * n / t / 1e9:.0f} GB/s of algorithmic bytes (76 B/atom)")
+
+
+if __name__ == "__main__":
+    _main()

@@ -94,7 +94,7 @@ int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, H
                     f.vx = (float)sg.vx; f.vy = (float)sg.vy; f.vz = (float)sg.vz;     // apex-relative
                     f.len = (float)sg.len;
                     f.tx = (float)sg.tx; f.ty = (float)sg.ty; f.tz = (float)sg.tz;
-                    f.wx = (float)sg.wx; f.wy = (float)sg.wy; f.wz = (float)sg.wz;
+                    f.wx = (float)(k1 * sg.wx); f.wy = (float)(k1 * sg.wy); f.wz = (float)(k1 * sg.wz);   // cK w
                     f.nx = (float)sg.nx; f.ny = (float)sg.ny; f.nz = (float)sg.nz;
                     recs.push_back(f);
                 }

@@ -44,10 +44,14 @@ struct AccF32K {
 // same reformulation as line_piece_fp64: the solid angle as the argument of
 // the product of unnormalised Van Oosterom-Strackee factors (renormalised
 // every 4 segments, well inside the FP32 range), e.(a x b) from the segment's
-// precomputed (A - apex) x (B - apex), cK folded into d.w.  d = a - sA t is
-// formed explicitly here (in FP32, |a|^2 - sA^2 would cancel).
+// precomputed (A - apex) x (B - apex), |d|^2 = |a|^2 - sA^2 and d.w = a.w
+// without forming d.  In FP32 |a|^2 - sA^2 loses digits for an atom near the
+// extension of a segment, but the term it enters carries d^2 through
+// d^2 K0 = sB/RB - sA/RA, so its absolute error stays below
+// cK |w| 2^-23 per segment.  The table holds w' = cK w, so d.w' is cK d.w and
+// the J0 term takes cJ / cK (cJK).
 __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const LineSegF* seg, float Px,
-                                                float Py, float Pz, float cJ, float cK,
+                                                float Py, float Pz, float cJK,
                                                 float& ux, float& uy, float& uz)
 {
     // apex = centre = origin of these coordinates
@@ -75,19 +79,19 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
         zr = nzr;
         const float sA = ax * s.tx + ay * s.ty + az * s.tz;
         const float sB = sA + s.len;
-        const float dx = ax - sA * s.tx, dy = ay - sA * s.ty, dz = az - sA * s.tz;
-        const float d2 = dx * dx + dy * dy + dz * dz;
-        const float dw = cK * (dx * s.wx + dy * s.wy + dz * s.wz);
+        const float d2 = fmaf(-sA, sA, la2);
+        const float dw = ax * s.wx + ay * s.wy + az * s.wz;          // cK d.w
         const float sum = la + lb;
-        const float ga = cJ * __logf(__fdividef(sum + s.len, sum - s.len));
+        const float ga = cJK * __logf(__fdividef(sum + s.len, sum - s.len));
         const float g = sB * ilb - sA * ila;
         const float al = d2 > 0.0f ? __fdividef(dw, d2) * g : 0.0f;
         const float be = dw * (ila - ilb);
-        lx += ga * s.wx - al * dx - be * s.tx;
-        ly += ga * s.wy - al * dy - be * s.ty;
-        lz += ga * s.wz - al * dz - be * s.tz;
+        const float c = fmaf(al, sA, -be);
+        lx = fmaf(c, s.tx, fmaf(-al, ax, fmaf(ga, s.wx, lx)));
+        ly = fmaf(c, s.ty, fmaf(-al, ay, fmaf(ga, s.wy, ly)));
+        lz = fmaf(c, s.tz, fmaf(-al, az, fmaf(ga, s.wz, lz)));
         ax = bx; ay = by; az = bz;
-        la = lb; ila = ilb;
+        la2 = lb2; la = lb; ila = ilb;
         ea = eb;
         if ((k & 3) == 3) {
             const float sc = __frcp_rn(fabsf(zr) + fabsf(zi));
@@ -151,7 +155,7 @@ struct LineFp32 {
     {
         const LinePieceF* pieces = reinterpret_cast<const LinePieceF*>(st);
         const LineSegF* recs = reinterpret_cast<const LineSegF*>(st + (size_t)npieces * sizeof(LinePieceF));
-        const float cJ = (float)a.cJ, cK = (float)a.cK;
+        const float cJK = (float)(a.cJ / a.cK);
         for (int p = 0; p < npieces; ++p) {
             const LinePieceF& pc = pieces[p];
             const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
@@ -161,7 +165,7 @@ struct LineFp32 {
                 const float Px = (float)(qx - sx), Py = (float)(qy - sy), Pz = (float)(qz - sz);
                 if (near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) continue;
                 float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-                line_piece_fp32(pc, recs + pc.rec, Px, Py, Pz, cJ, cK, fx, fy, fz);
+                line_piece_fp32(pc, recs + pc.rec, Px, Py, Pz, cJK, fx, fy, fz);
                 acc.add(fx, fy, fz);
             }
         }

@@ -9,8 +9,9 @@
   output scale).
 * What the network gains: trained here on exact far shells of random
   fcc_random-distribution loops, on held-out loops its error is a small
-  fraction of the truncated sum's (dropping the far shells) and it is many
-  times faster than the exact far-shell sum.
+  fraction of the truncated sum's (dropping the far shells), it is many times
+  faster than the exact far-shell sum, and faster than the far-field dipole
+  (one loopon of area A per loop), which is the more accurate approximation.
 * learned_displace: an untrained network fails the subsample check for every
   loop and the fallback reproduces the exact sum; a trained one passes.
 """
@@ -157,6 +158,18 @@ def test_network_gains_over_truncation_and_is_faster_than_exact():
     p.sync()
     t_net, t_exact = e0.elapsed_time(e1), e2.elapsed_time(e3)
     assert t_net * 20 < t_exact, (t_net, t_exact)
+    # the far-field dipole (one Kroupa loopon of area A per loop, cf. the far-field
+    # test of Code/tests/test_barnett.cpp) is more accurate but 702 loopon
+    # evaluations per (atom, loop): the network is faster
+    pd = B.Plan(Ln.dipole_loops(held), box, images=4, nu=0.34, image_min=2)
+    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e4.record()
+    pd.execute(big, u)
+    e5.record()
+    pd.sync()
+    t_dipole = e4.elapsed_time(e5)
+    assert t_net * 3 < t_dipole, (t_net, t_dipole)
+    assert r["dipole_max"] < r["truncation_max"], r
 
 
 def test_learned_displace_falls_back_and_matches_exact():

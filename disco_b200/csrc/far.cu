@@ -4,8 +4,9 @@
 // fallback).  The reference has no learned path; the exact sums it is checked
 // against and falls back to are the plan and batch forms of this library.
 //
-// Fused inference (far_kernel): one CTA of 128 threads owns a tile of 128 atoms
-// (thread t = row t = tensor-memory lane t) and walks the selected loops.  Per
+// Fused inference (far_kernel): one CTA of 256 threads owns a tile of 128 atoms
+// (row r = tensor-memory lane r; warps w and w + 4 read the same lanes and
+// split the 128 columns of each epilogue) and walks the selected loops.  Per
 // (tile, loop): the 16 features of each row go to shared memory as one BF16
 // K-major A tile; layer 1 is one 128x128x16 MMA, layers 2 and 3 eight MMAs of
 // K = 16 reading the previous activations from shared memory, layer 4 eight
@@ -53,7 +54,7 @@ constexpr uint32_t kImgBias = kImgW4 + kOut * kHid * 2;         // b1/2, b2/2, b
 constexpr uint32_t kImgBytes = kImgBias + (3 * kHid + kOut) * 4;
 static_assert(kImgBytes % 16 == 0, "bulk copies move multiples of 16 bytes");
 
-constexpr int kFarThreads = 128;
+constexpr int kFarThreads = 256;      // two threads per row: warps w and w + 4 split the columns
 constexpr uint32_t kSmX = (kImgBytes + 127) / 128 * 128;       // features tile [128 x 16]
 constexpr uint32_t kSmH = kSmX + 128 * kIn * 2;                 // activations [128 x 128]
 constexpr uint32_t kSmBar = kSmH + 128 * kHid * 2;
@@ -160,12 +161,12 @@ __device__ __forceinline__ bool mma_step(uint32_t tmem, uint32_t a_addr, uint32_
     return !bad;
 }
 
-// Hidden-layer epilogue of row `row`: H[row, :] = SiLU(acc + b) in BF16
-// (acc and bh hold halves: h = u + u tanh(u)).
-__device__ __forceinline__ void epilogue_hidden(uint32_t taddr, const float* bh, unsigned char* H, int row)
+// Hidden-layer epilogue of row `row`, columns [c0, c0 + 64): H[row, c] =
+// SiLU(acc + b) in BF16 (acc and bh hold halves: h = u + u tanh(u)).
+__device__ __forceinline__ void epilogue_hidden(uint32_t taddr, const float* bh, unsigned char* H, int row, int c0)
 {
 #pragma unroll 1
-    for (int c = 0; c < kHid; c += 32) {
+    for (int c = c0; c < c0 + kHid / 2; c += 32) {
         float v[32];
         tc::ld32(taddr + c, v);
         uint32_t w[16];
@@ -209,58 +210,69 @@ __global__ void __launch_bounds__(kFarThreads, 2) far_kernel(const FarArgs a)
                    aW4 = smem_addr(sm + kImgW4), aX = smem_addr(X), aH = smem_addr(H);
     constexpr uint32_t lbo128 = (128 / 8) * 128, lbo16 = (16 / 8) * 128;
     const uint32_t id_hid = tc::idesc_bf16(128, kHid), id_out = tc::idesc_bf16(128, kOut);
-    const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+    // warp w reads tensor-memory lanes 32 (w % 4) ...; warps 0-3 (half 0) own
+    // the rows' features and outputs, both halves share the epilogues
+    const int row = t & 127, half = t >> 7;
+    const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
     uint32_t phase = 0;
 
     for (int tile = blockIdx.x; ok && tile < a.ntiles; tile += gridDim.x) {
-        const int64_t atom = (int64_t)tile * 128 + t;
+        const int64_t atom = (int64_t)tile * 128 + row;
         const bool valid = atom < a.n;
-        const int64_t ia = valid ? atom : a.n - 1;
-        const double px = a.x[ia], py = a.y[ia], pz = a.z[ia];
+        double px = 0.0, py = 0.0, pz = 0.0;
+        if (half == 0) {
+            const int64_t ia = valid ? atom : a.n - 1;
+            px = a.x[ia]; py = a.y[ia]; pz = a.z[ia];
+        }
         float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-        FarLoop L = a.loops[a.sel[0]];
+        FarLoop L;
+        if (half == 0) L = a.loops[a.sel[0]];
         for (int s = 0; s < a.nsel; ++s) {
-            // the next loop's descriptor loads while this loop's layers run
-            const FarLoop next = a.loops[a.sel[s + 1 < a.nsel ? s + 1 : s]];
-            {
+            FarLoop next;
+            if (half == 0) {
+                // the next loop's descriptor loads while this loop's layers run
+                next = a.loops[a.sel[s + 1 < a.nsel ? s + 1 : s]];
                 float f[16];
                 features(px, py, pz, L, a.fn, f);
                 uint32_t w[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) w[i] = pack_bf16(f[2 * i], f[2 * i + 1]);
-                *reinterpret_cast<uint4*>(X + tc::kmajor_offset(t, 0, 128)) = make_uint4(w[0], w[1], w[2], w[3]);
-                *reinterpret_cast<uint4*>(X + tc::kmajor_offset(t, 8, 128)) = make_uint4(w[4], w[5], w[6], w[7]);
+                *reinterpret_cast<uint4*>(X + tc::kmajor_offset(row, 0, 128)) = make_uint4(w[0], w[1], w[2], w[3]);
+                *reinterpret_cast<uint4*>(X + tc::kmajor_offset(row, 8, 128)) = make_uint4(w[4], w[5], w[6], w[7]);
             }
             ok = mma_step(tmem, aX, lbo128, aW1, lbo128, kIn / 16, id_hid, &bar[1], phase);
             if (!ok) break;
-            epilogue_hidden(trow, bias, H, t);
+            epilogue_hidden(trow, bias, H, row, half * (kHid / 2));
             ok = mma_step(tmem, aH, lbo128, aW2, lbo128, kHid / 16, id_hid, &bar[1], phase);
             if (!ok) break;
-            epilogue_hidden(trow, bias + kHid, H, t);
+            epilogue_hidden(trow, bias + kHid, H, row, half * (kHid / 2));
             ok = mma_step(tmem, aH, lbo128, aW3, lbo128, kHid / 16, id_hid, &bar[1], phase);
             if (!ok) break;
-            epilogue_hidden(trow, bias + 2 * kHid, H, t);
+            epilogue_hidden(trow, bias + 2 * kHid, H, row, half * (kHid / 2));
             ok = mma_step(tmem, aH, lbo128, aW4, lbo16, kHid / 16, id_out, &bar[1], phase);
             if (!ok) break;
-            float y[16];
-            tc::ld16(trow, y);
-            const float* b4 = bias + 3 * kHid;
-            const float gx = (y[0] + b4[0]) * L.gain, gy = (y[1] + b4[1]) * L.gain, gz = (y[2] + b4[2]) * L.gain;
-            if (a.per_loop) {
-                if (valid) {
-                    float* o = a.per_loop + (int64_t)s * 3 * a.n;
-                    o[atom] = gx;
-                    o[a.n + atom] = gy;
-                    o[2 * a.n + atom] = gz;
+            if (half == 0) {
+                float y[16];
+                tc::ld16(trow, y);
+                const float* b4 = bias + 3 * kHid;
+                const float gx = (y[0] + b4[0]) * L.gain, gy = (y[1] + b4[1]) * L.gain,
+                            gz = (y[2] + b4[2]) * L.gain;
+                if (a.per_loop) {
+                    if (valid) {
+                        float* o = a.per_loop + (int64_t)s * 3 * a.n;
+                        o[atom] = gx;
+                        o[a.n + atom] = gy;
+                        o[2 * a.n + atom] = gz;
+                    }
+                } else {
+                    sx += gx;
+                    sy += gy;
+                    sz += gz;
                 }
-            } else {
-                sx += gx;
-                sy += gy;
-                sz += gz;
+                L = next;
             }
-            L = next;
         }
-        if (ok && valid && !a.per_loop) {
+        if (ok && half == 0 && valid && !a.per_loop) {
             a.ux[atom] += sx;
             a.uy[atom] += sy;
             a.uz[atom] += sz;

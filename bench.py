@@ -72,6 +72,50 @@ def dist_env():
         int(os.environ.get("LOCAL_RANK", 0))
 
 
+L2_BYTES = 126 * 2 ** 20
+
+
+class L2Flush:
+    """Rewrites a 256 MB buffer (twice the L2) between timed steps when a
+    workload's inputs would fit in L2; a no-op otherwise."""
+
+    def __init__(self, torch, input_bytes):
+        self.on = input_bytes < L2_BYTES
+        self.buf = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda") if self.on else None
+
+    def __call__(self):
+        if self.on:
+            self.buf.fill_(1)
+
+    def note(self, input_bytes):
+        return (f"L2 flushed between timed steps (inputs {input_bytes / 1e6:.0f} MB < L2)" if self.on else
+                f"inputs larger than L2 ({input_bytes / 1e6:.0f} MB)")
+
+
+def timed_steps(torch, step, steps, stream, flush):
+    """Device seconds of `steps` calls of step() (CUDA events on the launching
+    stream); with an active flush, L2 is rewritten before each step outside
+    the events."""
+    if not flush.on:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+    total = 0.0
+    for _ in range(steps):
+        flush()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1) * 1e-3
+    return total
+
+
 def measured_peaks():
     """The pool's measured peaks (HBM copy GB/s, BF16 TFLOP/s) from
     MEASURED_PEAKS.json beside this file, or None."""
@@ -252,11 +296,56 @@ def cpu_baseline(w, seconds, use_reference):
             "seconds": dt}, idx, u
 
 
+def run_reference_batch(args):
+    """Reference arm of the batch workload: the oracle restatement of kroupaCPU
+    (the reference has no batched form: it runs samples one after another) on
+    bounded samples of random batch samples, all host threads; the rate in
+    evaluations/s is converted to atoms/s of the whole batch."""
+    from disco_b200 import workloads as W
+    import oracle as O
+    threads = os.cpu_count() or 1
+    batch = W.batch(nsamples=args.samples)
+    n = sum(w.n for w in batch)
+    evals = sum(w.n * w.evals_per_atom() for w in batch)
+    rng = np.random.default_rng(99)
+    per_step = max(8.0, min(25.0, 150.0 / max(1, args.steps + args.warmup)))
+    times, done = [], []
+    for s in range(args.warmup + args.steps):
+        t_used, e_done = 0.0, 0.0
+        while t_used < per_step:
+            w = batch[rng.integers(len(batch))]
+            k = min(w.n, max(8, int(2e8 / max(1.0, w.evals_per_atom()))))
+            idx = np.sort(rng.choice(w.n, size=k, replace=False))
+            t0 = time.perf_counter()
+            O.displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box, images=w.images, nu=w.nu, threads=threads)
+            t_used += time.perf_counter() - t0
+            e_done += k * w.evals_per_atom()
+        if s >= args.warmup:
+            times.append(t_used)
+            done.append(e_done)
+    rate = sum(done) / sum(times)
+    value = rate * n / evals
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "batch", "samples": len(batch), "atoms": n, "evals_per_step": evals},
+        "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": threads, "kind": "port",
+                         "sample": f"random atoms of random samples, {per_step:.0f} s per step; evaluations/s "
+                                   "converted to the whole batch's atoms"},
+        "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    w = build_workload(args.config, args.images)
+    if args.config == "batch":
+        return run_reference_batch(args)
+    # the learned workload's reference is the exact sum over all 729 images (+-4)
+    w = build_workload("fcc_random", 4) if args.config == "learned" else build_workload(args.config, args.images)
     import oracle as O
     threads = os.cpu_count() or 1
     ref_ok = w.images == 1 and O.have_ref()
@@ -392,18 +481,14 @@ def run_ours(args):
     for _ in range(args.warmup):
         plan.execute(pos, u)
     plan.sync(stream.cuda_stream)
+    flush = L2Flush(torch, 48 * n)
     clocks = Clocks(local)
     barrier()
     clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        plan.execute(pos, u)
-    e1.record(stream)
+    elapsed = timed_steps(torch, lambda: plan.execute(pos, u), args.steps, stream, flush)
     barrier()
     clk = clocks.stop()
     plan.sync(stream.cuda_stream)
-    elapsed = e0.elapsed_time(e1) * 1e-3
     elapsed = max_over_ranks(elapsed, world)
     per_launch = elapsed / args.steps
     value = n * world * args.steps / elapsed
@@ -465,8 +550,8 @@ def run_ours(args):
             "config": {"workload": args.config, "atoms": n, "loops": len(w.loops),
                        "segments": st["n_segments"], "loopons": st["n_loopons"],
                        "images": st["n_images"], "nu": w.nu, "method": w.method,
-                       "precision": args.precision, "l2": "inputs larger than L2 (positions "
-                       f"{24 * n / 1e6:.0f} MB)", "parallelism": f"replicas x{world}"},
+                       "precision": args.precision, "l2": flush.note(48 * n),
+                       "parallelism": f"replicas x{world}"},
             "evals_per_s": evals_atom * n * world * args.steps / elapsed,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps, "parity": parity, "output": output,
@@ -792,19 +877,14 @@ def compaction_rate(lib, C, torch, stream):
         call()
     torch.cuda.synchronize()
     reps = 10
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        call()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t = e0.elapsed_time(e1) * 1e-3 / reps
+    flush = L2Flush(torch, 0)                     # always: 100 MB of positions, read twice
+    t = timed_steps(torch, call, reps, stream, flush) / reps
     pk = measured_peaks()
     peak = pk["hbm_gbs"] if pk else 6650.0
     gbs = 76.0 * n / t / 1e9
     return {"atoms": n, "survivors": int(counts[0]), "slab_atoms": int(counts[1]), "copies": int(counts[2]),
             "ms": 1e3 * t, "atoms_per_s": n / t, "algorithmic_bytes": 76 * n, "achieved_gbs": gbs,
-            "peak_gbs": peak, "frac": gbs / peak,
+            "peak_gbs": peak, "frac": gbs / peak, "l2": "flushed before each timed call",
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk else "fallback 6650 GB/s"}
 
 
@@ -877,18 +957,20 @@ def run_prismatic(args):
     for _ in range(args.warmup):
         step()
     plan.sync(stream.cuda_stream)
+    flush = L2Flush(torch, 48 * n)
+    kn = [0, 0]
+
+    def timed_step():
+        kn[0], kn[1] = step()
+
     clocks = Clocks(local)
     barrier()
     clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        k, nc = step()
-    e1.record(stream)
+    elapsed = timed_steps(torch, timed_step, args.steps, stream, flush)
     barrier()
     clk = clocks.stop()
     plan.sync(stream.cuda_stream)
-    elapsed = e0.elapsed_time(e1) * 1e-3
+    k, nc = kn
     elapsed = max_over_ranks(elapsed, world)
     per = elapsed / args.steps
     evals = st_plan["evals_per_atom"] * k
@@ -943,8 +1025,7 @@ def run_prismatic(args):
                        "loops": len(w.loops), "loopons": st_plan["n_loopons"], "images": st_plan["n_images"],
                        "nu": w.nu, "method": "loopons", "precision": args.precision,
                        "step": "matter step + loopon field + copy/add-u/wrap epilogue, all on device",
-                       "l2": "inputs fit in L2 (10 MB of positions); no flush (compute-bound: the "
-                             "field is >99 % of the step)", "parallelism": f"replicas x{world}"},
+                       "l2": flush.note(48 * n), "parallelism": f"replicas x{world}"},
             "evals_per_s": evals * world / per,
             "roofline": {"bound": "fp64" if prec == C.DISCO_FP64 else "fp32", "kernel": "loopon field",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,

@@ -181,35 +181,41 @@ __device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineS
 }
 
 // Field at P (atom - reference point - image shift) of one loopon piece:
-// Code/kroupa.hpp:52-73 with 1/rho from one rsqrt and m.rho, n.rho from
-// per-loopon projections.
+// Code/kroupa.hpp:52-73 regrouped.  With ir = 1/rho, mr = m.rho, nr = n.rho:
+//   du = fac fb (k2 (n mr + m nr - rho b_n) + tail rho),  k2 = c2 ir,
+//   tail = 3 mr nr ir^3,  fac = ir^2 (0 for rho < 1e-10)
+// is fac fb (alpha n + beta m + gamma rho) with alpha = c2 ir mr,
+// beta = c2 ir nr, gamma = ir (3 mr nr ir^2 - c2 b_n); fb factors out of the
+// sum over the piece's loopons.  1/rho from the kernels' own rsqrt.
 __device__ __forceinline__ void loopon_piece_fp64(const LooponPiece& pc, const LooponRec* __restrict__ rec,
                                                   double Px, double Py, double Pz, double c2,
                                                   double& ux, double& uy, double& uz)
 {
     const double mP = pc.mx * Px + pc.my * Py + pc.mz * Pz;
     const double nP = pc.nx * Px + pc.ny * Py + pc.nz * Pz;
+    const double c2bn = c2 * pc.b_n;
     double dx = 0.0, dy = 0.0, dz = 0.0;
     const int n = pc.n;
+#pragma unroll 2
     for (int k = 0; k < n; ++k) {
         const LooponRec l = rec[k];
         const double rx = Px - l.x, ry = Py - l.y, rz = Pz - l.z;
         const double r2 = rx * rx + ry * ry + rz * rz;
         const bool keep = r2 >= 1e-20;                           // rho >= 1e-10 (kroupa.hpp:55)
-        const double ir = rsqrt(keep ? r2 : 1.0);
+        const double ir = rsqrt_nr(keep ? r2 : 1.0);
         const double ir2 = ir * ir;
         const double mr = mP - l.ml, nr = nP - l.nl;
-        const double k2 = c2 * ir;
-        const double tail = 3.0 * mr * nr * (ir2 * ir);
+        const double cir = c2 * ir;
+        const double al = cir * mr, be = cir * nr;
+        const double ga = ir * fma(3.0 * mr * nr, ir2, -c2bn);
         const double fac = keep ? ir2 : 0.0;
-        const double ex = pc.nx * mr + pc.mx * nr - rx * pc.b_n;
-        const double ey = pc.ny * mr + pc.my * nr - ry * pc.b_n;
-        const double ez = pc.nz * mr + pc.mz * nr - rz * pc.b_n;
-        dx += fac * (pc.fbx * (k2 * ex + tail * rx));
-        dy += fac * (pc.fby * (k2 * ey + tail * ry));
-        dz += fac * (pc.fbz * (k2 * ez + tail * rz));
+        dx = fma(fac, fma(al, pc.nx, fma(be, pc.mx, ga * rx)), dx);
+        dy = fma(fac, fma(al, pc.ny, fma(be, pc.my, ga * ry)), dy);
+        dz = fma(fac, fma(al, pc.nz, fma(be, pc.mz, ga * rz)), dz);
     }
-    ux += dx; uy += dy; uz += dz;
+    ux = fma(pc.fbx, dx, ux);
+    uy = fma(pc.fby, dy, uy);
+    uz = fma(pc.fbz, dz, uz);
 }
 
 // ---- the two FP64 policies ----------------------------------------------------------------

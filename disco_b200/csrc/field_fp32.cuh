@@ -109,10 +109,13 @@ __device__ __forceinline__ void loopon_piece_fp32(const LooponPieceF& pc, const 
                                                   float Py, float Pz, float c2, float& ux, float& uy,
                                                   float& uz)
 {
+    // regrouped as loopon_piece_fp64: fb (alpha n + beta m + gamma rho) fac
     const float mP = pc.mx * Px + pc.my * Py + pc.mz * Pz;
     const float nP = pc.nx * Px + pc.ny * Py + pc.nz * Pz;
+    const float c2bn = c2 * pc.b_n;
     float dx = 0.0f, dy = 0.0f, dz = 0.0f;
     const int n = pc.n;
+#pragma unroll 2
     for (int k = 0; k < n; ++k) {
         const LooponRecF l = rec[k];
         const float rx = Px - l.x, ry = Py - l.y, rz = Pz - l.z;
@@ -121,17 +124,15 @@ __device__ __forceinline__ void loopon_piece_fp32(const LooponPieceF& pc, const 
         const float ir = rsqrtf(keep ? r2 : 1.0f);
         const float ir2 = ir * ir;
         const float mr = mP - l.ml, nr = nP - l.nl;
-        const float k2 = c2 * ir;
-        const float tail = 3.0f * mr * nr * (ir2 * ir);
+        const float cir = c2 * ir;
+        const float al = cir * mr, be = cir * nr;
+        const float ga = ir * fmaf(3.0f * mr * nr, ir2, -c2bn);
         const float fac = keep ? ir2 : 0.0f;
-        const float ex = pc.nx * mr + pc.mx * nr - rx * pc.b_n;
-        const float ey = pc.ny * mr + pc.my * nr - ry * pc.b_n;
-        const float ez = pc.nz * mr + pc.mz * nr - rz * pc.b_n;
-        dx += fac * (pc.fbx * (k2 * ex + tail * rx));
-        dy += fac * (pc.fby * (k2 * ey + tail * ry));
-        dz += fac * (pc.fbz * (k2 * ez + tail * rz));
+        dx = fmaf(fac, fmaf(al, pc.nx, fmaf(be, pc.mx, ga * rx)), dx);
+        dy = fmaf(fac, fmaf(al, pc.ny, fmaf(be, pc.my, ga * ry)), dy);
+        dz = fmaf(fac, fmaf(al, pc.nz, fmaf(be, pc.mz, ga * rz)), dz);
     }
-    ux += dx; uy += dy; uz += dz;
+    ux += pc.fbx * dx; uy += pc.fby * dy; uz += pc.fbz * dz;
 }
 
 // The near-cut test, shared by the FP32 pass (which skips what it selects)

@@ -705,7 +705,7 @@ def run_learned(args):
     2 <= max|n| <= 4 (702 images), the exact FP64 far-shell sum re-checked on a
     1 % stratified random atom subsample every step with per-loop fallback.
     The plain FP64 path on the same workload (all 729 images exact) is timed
-    once and judges the learned result on every atom."""
+    once and is the reference for the learned result on every atom."""
     import torch
     from disco_b200 import backend as B
     from disco_b200 import _capi as C

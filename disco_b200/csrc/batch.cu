@@ -1,5 +1,5 @@
 // Batched form: many independent samples (own atoms, loops, box, image range)
-// in one persistent launch per loop kind (SURVEY's disco_b200_batch).
+// in one persistent launch per loop kind.
 //
 // Work unit = (sample, atom tile, table chunk).  The host knows every unit's
 // exact cost (tile atoms x chunk segments or loopons x images), sorts the

@@ -193,7 +193,7 @@ typedef struct {
 
 typedef struct disco_batch_plan disco_batch_plan;
 
-/* Batched form of disco_b200_displace (SURVEY's disco_b200_batch): every sample's
+/* Batched form of disco_b200_displace: every sample's
  * field is added into its own u.  All samples run in one persistent launch per
  * loop kind over a queue of (sample, atom tile, table chunk) units, balanced
  * across the CTAs by their exact cost; opt->image_split and opt->stage_kb are

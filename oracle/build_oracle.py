@@ -13,6 +13,13 @@ Three shared libraries, all host code:
                                            oracle/ref_harness.cpp; built only where
                                            the reference tree exists
   oracle/_ref/libdisco_ref_nofma.so       the same with -ffp-contract=off
+  oracle/_ref/exec_b200                   the reference's own driver (Code/main.cpp
+                                           and its host sources, Code/Makefile's
+                                           SRC_HOST) compiled in place with
+                                           -DWITH_CUDA and linked with this
+                                           library's backend shim instead of
+                                           backend_cuda.cu; yaml-cpp, absent here,
+                                           is replaced by oracle/yaml_subset
 
 GCC contracts a*b+c into FMAs where it sees fit, and it does not contract the
 reference and the restatement identically (the reference folds nu = 0.35 at
@@ -39,6 +46,9 @@ ORACLE_SO = os.path.join(HERE, "_build", "libdisco_oracle.so")
 ORACLE_NOFMA_SO = os.path.join(HERE, "_build", "libdisco_oracle_nofma.so")
 REF_SO = os.path.join(HERE, "_ref", "libdisco_ref.so")
 REF_NOFMA_SO = os.path.join(HERE, "_ref", "libdisco_ref_nofma.so")
+REF_EXEC = os.path.join(HERE, "_ref", "exec_b200")
+HOST_SOURCES = ("main.cpp", "input.cpp", "loop.cpp", "loop_deform.cpp", "prismatic.cpp", "polycrystal.cpp",
+                "twin.cpp", "backend_cpu.cpp")
 
 
 def _stale(out, deps):
@@ -73,8 +83,26 @@ def build(force=False, verbose=True):
         if force or _stale(REF_NOFMA_SO, deps):
             _run([CXX, "-std=c++14", *BASE, "-ffp-contract=off", "-I", REF_CODE, harness, *ref_srcs,
                   "-o", REF_NOFMA_SO])
+        build_driver(force)
     elif verbose:
         print(f"reference tree {REF_CODE} absent: oracle/_ref not rebuilt", flush=True)
+
+
+def build_driver(force=False):
+    """The reference's driver, unchanged, on this library's backend (the
+    integration a maintainer would make, built here as a test harness)."""
+    lib = os.path.join(REPO, "disco_b200", "_lib")
+    shim = os.path.join(lib, "libdisco_backend.so")
+    if not os.path.exists(shim):
+        return
+    srcs = [os.path.join(REF_CODE, f) for f in HOST_SOURCES]
+    yaml_h = os.path.join(HERE, "yaml_subset", "yaml-cpp", "yaml.h")
+    hdrs = [os.path.join(REF_CODE, f) for f in os.listdir(REF_CODE) if f.endswith(".hpp")]
+    if force or _stale(REF_EXEC, [*srcs, *hdrs, yaml_h, shim, __file__]):
+        _run([CXX, "-std=c++14", "-O3", "-march=x86-64-v3", "-fopenmp", "-DWITH_CUDA",
+              "-I", os.path.join(HERE, "yaml_subset"), "-I", REF_CODE, *srcs,
+              "-L", lib, "-ldisco_backend", "-ldisco_b200", "-Wl,-rpath,$ORIGIN/../../disco_b200/_lib",
+              "-o", REF_EXEC])
 
 
 if __name__ == "__main__":

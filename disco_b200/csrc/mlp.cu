@@ -69,11 +69,82 @@ __device__ __forceinline__ float load_elem(const Operand& o, int64_t r, int64_t 
                            : __bfloat162float(static_cast<const __nv_bfloat16*>(o.ptr)[idx]);
 }
 
+__device__ __forceinline__ uint32_t bf16x2(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// 8 consecutive elements (along the row in memory) at p as 8 floats
+__device__ __forceinline__ void load8(const Operand& o, int64_t idx, float* v)
+{
+    if (o.dtype == kF32) {
+        const float4* q = reinterpret_cast<const float4*>(static_cast<const float*>(o.ptr) + idx);
+        const float4 a = q[0], b = q[1];
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    } else {
+        const uint4 u = *reinterpret_cast<const uint4*>(static_cast<const __nv_bfloat16*>(o.ptr) + idx);
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __bfloat1622float2(h[i]);
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    }
+}
+
+// Whole tile in range and 16-byte aligned along memory rows: 8-element vector
+// loads, and 16-byte shared stores of 8 K-consecutive values (transposed
+// operands: 8 x 8 blocks transposed in registers).  Rows vary fastest across
+// threads, so the stores of a warp fill whole 128-byte core matrices.
+__device__ __forceinline__ bool tile_fast(const Operand& o, int rows, int64_t r0, int64_t rmax, int64_t k0, int kc,
+                                          int64_t kmax)
+{
+    const int esz = o.dtype == kF32 ? 4 : 2;
+    const bool in = r0 + rows <= rmax && k0 + kc <= kmax && (kc % 8) == 0;
+    const bool al = ((reinterpret_cast<uintptr_t>(o.ptr) & 15) == 0) && ((o.ld * esz) % 16 == 0) &&
+                    (((o.transposed ? r0 : k0) * esz) % 16 == 0);
+    return in && al;
+}
+
+__device__ __forceinline__ void load_tile_fast(const Operand& o, unsigned char* base, int rows, int64_t r0,
+                                               int64_t k0, int kc)
+{
+    if (!o.transposed) {
+        const int total = rows * (kc / 8);
+        for (int e = threadIdx.x; e < total; e += kThreads) {
+            const int r = e % rows, k8 = (e / rows) * 8;
+            float v[8];
+            load8(o, (r0 + r) * o.ld + k0 + k8, v);
+            *reinterpret_cast<uint4*>(base + tc::kmajor_offset(r, k8, rows)) =
+                make_uint4(bf16x2(v[0], v[1]), bf16x2(v[2], v[3]), bf16x2(v[4], v[5]), bf16x2(v[6], v[7]));
+        }
+    } else {
+        const int total = (rows / 8) * (kc / 8);
+        for (int e = threadIdx.x; e < total; e += kThreads) {
+            const int r8 = (e % (rows / 8)) * 8, k8 = (e / (rows / 8)) * 8;
+            float v[8][8];                   // v[k][r]
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) load8(o, (k0 + k8 + kk) * o.ld + r0 + r8, v[kk]);
+#pragma unroll
+            for (int rr = 0; rr < 8; ++rr)
+                *reinterpret_cast<uint4*>(base + tc::kmajor_offset(r8 + rr, k8, rows)) =
+                    make_uint4(bf16x2(v[0][rr], v[1][rr]), bf16x2(v[2][rr], v[3][rr]), bf16x2(v[4][rr], v[5][rr]),
+                               bf16x2(v[6][rr], v[7][rr]));
+        }
+    }
+}
+
 // rows x kc tile of an operand into shared memory (K-major, BF16), zero-padded
 __device__ __forceinline__ void load_tile(const Operand& o, __nv_bfloat16* smem, int rows, int64_t r0, int64_t rmax,
                                           int64_t k0, int kc, int64_t kmax)
 {
     unsigned char* base = reinterpret_cast<unsigned char*>(smem);
+    if (tile_fast(o, rows, r0, rmax, k0, kc, kmax)) {
+        load_tile_fast(o, base, rows, r0, k0, kc);
+        return;
+    }
     const int total = rows * kc;
     if (!o.transposed) {
         for (int e = threadIdx.x; e < total; e += kThreads) {

@@ -366,16 +366,44 @@ def _main():
     """python -m disco_b200.learned far --atoms N --loops L [--reps R]: the fused
     far kernel on a seeded case (random-init network, fcc_random-distribution
     loops, atoms uniform in the 150^3 FCC box), timed with CUDA events; the
-    case the far kernel's ncu summaries are taken on."""
+    case the far kernel's ncu summaries are taken on.
+    python -m disco_b200.learned train [--batch B] [--reps R]: training steps
+    (forward, backward, Adam) on seeded random data, timed the same way."""
     import argparse
     import torch
     from . import workloads as W
     p = argparse.ArgumentParser()
-    p.add_argument("what", choices=["far"])
+    p.add_argument("what", choices=["far", "train"])
     p.add_argument("--atoms", type=int, default=131072)
     p.add_argument("--loops", type=int, default=64)
     p.add_argument("--reps", type=int, default=3)
+    p.add_argument("--batch", type=int, default=4096)
     a = p.parse_args()
+    if a.what == "train":
+        # training steps on seeded random data: per-step time of grad + Adam
+        torch.manual_seed(0)
+        X = torch.zeros((a.batch * 8, 16), dtype=torch.float32, device="cuda")
+        X[:, :14].uniform_(-1, 1)
+        T = torch.stack([torch.sin(2 * X[:, 0]) * X[:, 3], X[:, 1] * X[:, 2], torch.cos(X[:, 4] + X[:, 5])], 1)
+        m = MLP(seed=1)
+        for i in range(8):
+            m.grad(X[i * a.batch:(i + 1) * a.batch], T[i * a.batch:(i + 1) * a.batch], want_loss=False)
+            m.adam(lr=1e-3)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.time()
+        e0.record()
+        for k in range(a.reps):
+            i = k % 8
+            m.grad(X[i * a.batch:(i + 1) * a.batch], T[i * a.batch:(i + 1) * a.batch], want_loss=False)
+            m.adam(lr=1e-3)
+        e1.record()
+        torch.cuda.synchronize()
+        wall = time.time() - t0
+        m.status()
+        print(f"training step (batch {a.batch}): {e0.elapsed_time(e1) / a.reps:.3f} ms device, "
+              f"{1e3 * wall / a.reps:.3f} ms wall per step")
+        return
     L = 150 * 3.615
     box = (L, L, L)
     loops = W.fcc_random_loops(a.loops, 2)

@@ -156,3 +156,37 @@ def test_full_size_subsample(name):
     g = _gpu(w)
     ref = _oracle(w, atoms=(w.x[idx], w.y[idx], w.z[idx]))
     assert np.abs(g[idx] - ref).max() <= TOL
+
+
+def test_largest_image_range_and_orthorhombic_box():
+    """images = 8 (17^3 images, the largest the C-ABI takes) in a box with
+    three different edges, line and loopon methods."""
+    rng = np.random.default_rng(8)
+    loops = W.fcc_random_loops(3, 8, cells=6, a0=3.615)
+    box = (6 * 3.615, 5 * 3.615, 7 * 3.615)
+    pos = rng.uniform(-0.5, 0.5, size=(3, 40)) * np.array(box)[:, None]
+    w = W.Workload("ortho", pos[0], pos[1], pos[2], loops, box, 8, 0.31, "line")
+    assert np.abs(_gpu(w) - _oracle(w)).max() <= TOL
+    p = W.bcc_prismatic(cells=5, rmin=3.0, rmax=4.0, n_inter=1, n_vac=1)
+    wp = W.Workload("ortho_loopons", pos[0], pos[1], pos[2], p.loops, box, 8, 0.28, "loopons")
+    assert np.abs(_gpu(wp) - _oracle(wp)).max() <= TOL
+
+
+def test_far_field_series_tiers_and_logarithm():
+    """Atoms from 0.5 A to 2 km from one long-sided rectangle and one fine
+    circle: every J0 path (logarithm, 8-, 6- and 4-term series) against the
+    oracle, which always takes the logarithm."""
+    from disco_b200 import geometry as G
+    rect = G.Loop.rectangle(1.0, 30.0, 12.0, 0.0, (0.0, 0.0, 0.0), (1, -1, 0), (1, 1, 1), 3.615)
+    circ = G.Loop.circle(1.0, 20.0, (0.0, 0.0, 0.0), (1, -1, 0), (1, 1, 1), 3.615)
+    loops = [rect.line_data(vertices=rect.polyline(0.01)),
+             circ.line_data(vertices=circ.polyline(G.circle_eps_for_chords(20.0, 48)))]
+    r = np.concatenate([np.geomspace(0.5, 2.0e4, 300), np.geomspace(0.5, 2.0e4, 300)])
+    rng = np.random.default_rng(9)
+    d = rng.normal(size=(3, len(r)))
+    d /= np.linalg.norm(d, axis=0)
+    pos = d * r
+    box = (1.0e5, 1.0e5, 1.0e5)
+    w = W.Workload("tiers", pos[0], pos[1], pos[2], loops, box, 0, 0.34, "line")
+    got, ref = _gpu(w), _oracle(w)
+    assert np.abs(got - ref).max() <= TOL

@@ -564,7 +564,7 @@ def run_ours(args):
 
 
 def run_batch(args):
-    """Config 4: 256 independent BCC samples in one persistent, graph-captured
+    """The batch workload: 256 independent BCC samples in one persistent, graph-captured
     launch (FP32 compensated by default), knobs from the autotuner."""
     import torch
     import torch.distributed as dist
@@ -598,18 +598,14 @@ def run_batch(args):
     for _ in range(args.warmup):
         plan.execute(stream.cuda_stream)
     plan.sync(stream.cuda_stream)
+    flush = L2Flush(torch, 48 * n)
     clocks = Clocks(local)
     barrier()
     clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        plan.execute(stream.cuda_stream)
-    e1.record(stream)
+    elapsed = timed_steps(torch, lambda: plan.execute(stream.cuda_stream), args.steps, stream, flush)
     barrier()
     clk = clocks.stop()
     plan.sync(stream.cuda_stream)
-    elapsed = e0.elapsed_time(e1) * 1e-3
     elapsed = max_over_ranks(elapsed, world)
     per = elapsed / args.steps
     # parity: a fresh sum on a few samples against the oracle
@@ -685,7 +681,7 @@ def run_batch(args):
                        "tuning": {"image_split": tune["image_split"], "stage_kb": tune["stage_kb"],
                                   "stages": tune["stages"]},
                        "graph": "one CUDA graph replay per step",
-                       "l2": f"inputs larger than L2 ({24 * n / 1e9:.2f} GB of positions)",
+                       "l2": flush.note(48 * n),
                        "parallelism": f"replicas x{world}"},
             "evals_per_s": evals * world / per,
             "roofline": roof,
@@ -889,7 +885,7 @@ def compaction_rate(lib, C, torch, stream):
 
 
 def run_prismatic(args):
-    """Config 3: one step = the prismatic matter step (slab selection, vacancy
+    """The bcc_prismatic workload: one step = the prismatic matter step (slab selection, vacancy
     removal, interstitial copies; disco_b200_prismatic_noalloc on device
     arrays), the loopon field of all 16 loops over the surviving atoms (plan),
     and the fused copy/add-u/wrap epilogue (disco_b200_finalize_resident).

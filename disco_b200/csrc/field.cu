@@ -58,7 +58,7 @@ int build_table(const disco_loop* loops, int nloops, int kind, int precision, do
                 const int k1e = std::min(nv, k0 + kMaxLinePiece);
                 LinePiece p;
                 std::vector<LineSeg> recs;
-                make_line_piece(lp, k0, k1e, bx, by, bz, p, recs);
+                make_line_piece(lp, k0, k1e, bx, by, bz, k1, p, recs);
                 L.pieces.push_back(p);
                 L.recs.push_back(std::move(recs));
             }

@@ -91,14 +91,16 @@ __device__ __forceinline__ unsigned series_tier(double lmax, double gap2)
 // positive factor la lb does not change the argument), renormalised every 16
 // segments.  With d = a - sA t: |d|^2 = |a|^2 - sA^2 and d.w = a.w (w = b x t
 // is orthogonal to t), so d is never formed; its term -al d enters as
-// -al a + al sA t.  cK is folded into d.w, 2 cJ into the J0 factor.
+// -al a + al sA t.  The table holds w' = cK w, so a.w' is cK d.w, and the J0
+// term takes cJ / cK (cJK; 2 cJK for the half series).  The K0 term's d^2 > 0
+// test reads the sign and zero of d^2 from its bits (integer pipe).
 template <int NS>
 __device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, double rx, double ry, double rz,
                                               double ex, double ey, double ez, double ax, double ay, double az,
-                                              double cJ, double cK, double& zr, double& zi,
+                                              double cJK, double& zr, double& zi,
                                               double& lx, double& ly, double& lz)
 {
-    const double c2J = 2.0 * cJ;
+    const double c2J = 2.0 * cJK;
     double la2 = ax * ax + ay * ay + az * az;
     double ila = rsqrt_nr(la2);
     double la = la2 * ila;
@@ -124,13 +126,13 @@ __device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, doub
         const double sA = ax * s.tx + ay * s.ty + az * s.tz;
         const double sB = sA + s.len;
         const double d2 = fma(-sA, sA, la2);
-        const double dw = cK * (ax * s.wx + ay * s.wy + az * s.wz);      // cK d.w
+        const double dw = ax * s.wx + ay * s.wy + az * s.wz;             // cK d.w
         const double sum = la + lb;
         double ga;
         if (NS > 0) ga = c2J * half_j0_series<NS>(s.len * rcp_nr(sum));
-        else        ga = cJ * log((sum + s.len) * rcp_nr(sum - s.len));
+        else        ga = cJK * log((sum + s.len) * rcp_nr(sum - s.len));
         const double g = sB * ilb - sA * ila;                           // d^2 K0
-        const double al = d2 > 0.0 ? dw * rcp_nr(d2) * g : 0.0;
+        const double al = __double_as_longlong(d2) > 0 ? dw * rcp_nr(d2) * g : 0.0;
         const double be = dw * (ila - ilb);                             // cK d.w K1
         const double c = fma(al, sA, -be);
         lx = fma(c, s.tx, fma(-al, ax, fma(ga, s.wx, lx)));
@@ -154,7 +156,7 @@ __device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, doub
 // RA + RB >= 2 (l1 - rho) with l1 = |apex - P| and rho the piece's largest
 // vertex radius, so t = L/(RA+RB) <= lmax / (2 (l1 - rho)).
 __device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineSeg* seg,
-                                                double Px, double Py, double Pz, double cJ, double cK,
+                                                double Px, double Py, double Pz, double cJK,
                                                 double& ux, double& uy, double& uz)
 {
     // unit vector from P to the fan apex
@@ -169,10 +171,10 @@ __device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineS
     double zr = 1.0, zi = 0.0, lx = 0.0, ly = 0.0, lz = 0.0;
     const double ax = pc.ax + rx, ay = pc.ay + ry, az = pc.az + rz;
     switch (tier) {
-    case 3:  line_segments<4>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz); break;
-    case 2:  line_segments<6>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz); break;
-    case 1:  line_segments<8>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz); break;
-    default: line_segments<0>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJ, cK, zr, zi, lx, ly, lz); break;
+    case 3:  line_segments<4>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJK, zr, zi, lx, ly, lz); break;
+    case 2:  line_segments<6>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJK, zr, zi, lx, ly, lz); break;
+    case 1:  line_segments<8>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJK, zr, zi, lx, ly, lz); break;
+    default: line_segments<0>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJK, zr, zi, lx, ly, lz); break;
     }
     const double f = atan2(zi, zr) * (1.0 / 6.283185307179586476925286766559);   // Omega / (4 pi)
     ux += pc.bx * f + lx;
@@ -235,12 +237,13 @@ struct LineFp64 {
     {
         const LinePiece* pieces = reinterpret_cast<const LinePiece*>(st);
         const LineSeg* recs = reinterpret_cast<const LineSeg*>(st + (size_t)npieces * sizeof(LinePiece));
+        const double cJK = a.cJ / a.cK;
         for (int p = 0; p < npieces; ++p) {
             const LinePiece& pc = pieces[p];
             for (int img = split; img < a.nimg; img += S) {
                 double sx, sy, sz;
                 if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
-                line_piece_fp64(pc, recs + pc.rec, px - sx, py - sy, pz - sz, a.cJ, a.cK, acc.x, acc.y, acc.z);
+                line_piece_fp64(pc, recs + pc.rec, px - sx, py - sy, pz - sz, cJK, acc.x, acc.y, acc.z);
             }
         }
     }
@@ -367,9 +370,10 @@ __global__ void __launch_bounds__(kThreads, Policy::kMinBlocks) field_kernel(con
 
 // One FP64 line piece: segments k0..k1e-1 of loop lp (segment k runs from
 // vertex k-1 to vertex k; Code/barnett.hpp:62-65), with everything that does
-// not depend on the atom precomputed.  rec is left to the chunk packer.
+// not depend on the atom precomputed; w is stored times cK = 1/(8 pi (1 - nu)).
+// rec is left to the chunk packer.
 inline void make_line_piece(const disco_loop& lp, int k0, int k1e, double bx, double by, double bz,
-                            LinePiece& p, std::vector<LineSeg>& recs)
+                            double cK, LinePiece& p, std::vector<LineSeg>& recs)
 {
     const int nv = lp.n_vertices;
     std::memset(&p, 0, sizeof(p));
@@ -399,9 +403,9 @@ inline void make_line_piece(const disco_loop& lp, int k0, int k1e, double bx, do
         if (L > 0.0) {
             s.len = L;
             s.tx = tx / L; s.ty = ty / L; s.tz = tz / L;
-            s.wx = by * s.tz - bz * s.ty;
-            s.wy = bz * s.tx - bx * s.tz;
-            s.wz = bx * s.ty - by * s.tx;
+            s.wx = cK * (by * s.tz - bz * s.ty);
+            s.wy = cK * (bz * s.tx - bx * s.tz);
+            s.wz = cK * (bx * s.ty - by * s.tx);
         }
         p.rho = std::max(p.rho, radius(k));
         p.lmax = std::max(p.lmax, L);

@@ -75,7 +75,7 @@ int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, H
                 const int a = (k0 + nv - 1) % nv;
                 LinePiece q;
                 std::vector<LineSeg> segs;
-                make_line_piece(lp, k0, k1e, bx, by, bz, q, segs);
+                make_line_piece(lp, k0, k1e, bx, by, bz, k1, q, segs);
                 q.rec = (int32_t)s64.size();
                 LinePieceF p;
                 std::memset(&p, 0, sizeof(p));
@@ -94,7 +94,7 @@ int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, H
                     f.vx = (float)sg.vx; f.vy = (float)sg.vy; f.vz = (float)sg.vz;     // apex-relative
                     f.len = (float)sg.len;
                     f.tx = (float)sg.tx; f.ty = (float)sg.ty; f.tz = (float)sg.tz;
-                    f.wx = (float)(k1 * sg.wx); f.wy = (float)(k1 * sg.wy); f.wz = (float)(k1 * sg.wz);   // cK w
+                    f.wx = (float)sg.wx; f.wy = (float)sg.wy; f.wz = (float)sg.wz;      // cK w
                     f.nx = (float)sg.nx; f.ny = (float)sg.ny; f.nz = (float)sg.nz;
                     recs.push_back(f);
                 }

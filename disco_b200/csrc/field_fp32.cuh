@@ -40,6 +40,31 @@ struct AccF32K {
     }
 };
 
+// The hardware approximations with denormals flushed (single MUFU
+// operations; every argument here is a normal number: the near cut keeps an
+// atom at least near_h from the loop plane or near_r beyond its rim, and a
+// loopon's rho^2 is at least 1e-20).
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float rcp_ftz(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float lg2_ftz(float x)
+{
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Code/barnett.hpp:44-107 in FP32 on centre-relative coordinates, with the
 // same reformulation as line_piece_fp64: the solid angle as the argument of
 // the product of unnormalised Van Oosterom-Strackee factors (renormalised
@@ -49,17 +74,19 @@ struct AccF32K {
 // extension of a segment, but the term it enters carries d^2 through
 // d^2 K0 = sB/RB - sA/RA, so its absolute error stays below
 // cK |w| 2^-23 per segment.  The table holds w' = cK w, so d.w' is cK d.w and
-// the J0 term takes cJ / cK (cJK).
+// the J0 term takes cJ ln2 / cK (cJK2, with J0 from the base-2 logarithm).
+// The solid-angle renormalisation only needs some positive scale, so an
+// approximate reciprocal serves.
 __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const LineSegF* seg, float Px,
-                                                float Py, float Pz, float cJK,
+                                                float Py, float Pz, float cJK2,
                                                 float& ux, float& uy, float& uz)
 {
     // apex = centre = origin of these coordinates
-    const float il1 = rsqrtf(Px * Px + Py * Py + Pz * Pz);
+    const float il1 = rsqrt_ftz(Px * Px + Py * Py + Pz * Pz);
     const float ex = -Px * il1, ey = -Py * il1, ez = -Pz * il1;
     float ax = pc.ax - Px, ay = pc.ay - Py, az = pc.az - Pz;
     float la2 = ax * ax + ay * ay + az * az;
-    float ila = rsqrtf(la2);
+    float ila = rsqrt_ftz(la2);
     float la = la2 * ila;
     float ea = ex * ax + ey * ay + ez * az;
     float zr = 1.0f, zi = 0.0f, lx = 0.0f, ly = 0.0f, lz = 0.0f;
@@ -69,7 +96,7 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
         const LineSegF s = seg[k];
         const float bx = s.vx - Px, by = s.vy - Py, bz = s.vz - Pz;
         const float lb2 = bx * bx + by * by + bz * bz;
-        const float ilb = rsqrtf(lb2);
+        const float ilb = rsqrt_ftz(lb2);
         const float lb = lb2 * ilb;
         const float eb = ex * bx + ey * by + ez * bz;
         const float den = fmaf(ea, lb, fmaf(eb, la, fmaf(la, lb, ax * bx + ay * by + az * bz)));
@@ -82,9 +109,9 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
         const float d2 = fmaf(-sA, sA, la2);
         const float dw = ax * s.wx + ay * s.wy + az * s.wz;          // cK d.w
         const float sum = la + lb;
-        const float ga = cJK * __logf(__fdividef(sum + s.len, sum - s.len));
+        const float ga = cJK2 * lg2_ftz((sum + s.len) * rcp_ftz(sum - s.len));
         const float g = sB * ilb - sA * ila;
-        const float al = d2 > 0.0f ? __fdividef(dw, d2) * g : 0.0f;
+        const float al = d2 > 0.0f ? dw * rcp_ftz(d2) * g : 0.0f;
         const float be = dw * (ila - ilb);
         const float c = fmaf(al, sA, -be);
         lx = fmaf(c, s.tx, fmaf(-al, ax, fmaf(ga, s.wx, lx)));
@@ -94,7 +121,7 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
         la2 = lb2; la = lb; ila = ilb;
         ea = eb;
         if ((k & 3) == 3) {
-            const float sc = __frcp_rn(fabsf(zr) + fabsf(zi));
+            const float sc = rcp_ftz(fabsf(zr) + fabsf(zi));
             zr *= sc; zi *= sc;
         }
     }
@@ -121,7 +148,7 @@ __device__ __forceinline__ void loopon_piece_fp32(const LooponPieceF& pc, const 
         const float rx = Px - l.x, ry = Py - l.y, rz = Pz - l.z;
         const float r2 = rx * rx + ry * ry + rz * rz;
         const bool keep = r2 >= 1e-20f;
-        const float ir = rsqrtf(keep ? r2 : 1.0f);
+        const float ir = rsqrt_ftz(keep ? r2 : 1.0f);
         const float ir2 = ir * ir;
         const float mr = mP - l.ml, nr = nP - l.nl;
         const float cir = c2 * ir;
@@ -156,7 +183,7 @@ struct LineFp32 {
     {
         const LinePieceF* pieces = reinterpret_cast<const LinePieceF*>(st);
         const LineSegF* recs = reinterpret_cast<const LineSegF*>(st + (size_t)npieces * sizeof(LinePieceF));
-        const float cJK = (float)(a.cJ / a.cK);
+        const float cJK2 = (float)(a.cJ / a.cK * 0.69314718055994530942);
         for (int p = 0; p < npieces; ++p) {
             const LinePieceF& pc = pieces[p];
             const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
@@ -166,7 +193,7 @@ struct LineFp32 {
                 const float Px = (float)(qx - sx), Py = (float)(qy - sy), Pz = (float)(qz - sz);
                 if (near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) continue;
                 float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-                line_piece_fp32(pc, recs + pc.rec, Px, Py, Pz, cJK, fx, fy, fz);
+                line_piece_fp32(pc, recs + pc.rec, Px, Py, Pz, cJK2, fx, fy, fz);
                 acc.add(fx, fy, fz);
             }
         }
@@ -182,6 +209,7 @@ struct LineNearFp64 {
                                                  int split, double px, double py, double pz, Acc& acc)
     {
         const LinePieceF* pieces = reinterpret_cast<const LinePieceF*>(st);
+        const double cJK = a.cJ / a.cK;
         for (int p = 0; p < npieces; ++p) {
             const LinePieceF& pc = pieces[p];
             const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
@@ -191,7 +219,7 @@ struct LineNearFp64 {
                 const float Px = (float)(qx - sx), Py = (float)(qy - sy), Pz = (float)(qz - sz);
                 if (!near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) continue;
                 const LinePiece& p64 = a.pieces64[pc.piece64];
-                line_piece_fp64(p64, a.segs64 + p64.rec, px - sx, py - sy, pz - sz, a.cJ, a.cK,
+                line_piece_fp64(p64, a.segs64 + p64.rec, px - sx, py - sy, pz - sz, cJK,
                                 acc.x, acc.y, acc.z);
             }
         }

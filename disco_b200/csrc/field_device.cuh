@@ -105,7 +105,7 @@ __device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, doub
     double ila = rsqrt_nr(la2);
     double la = la2 * ila;
     double ea = ex * ax + ey * ay + ez * az;                            // e . a
-#pragma unroll 2
+#pragma unroll 4
     for (int k = 0; k < nseg; ++k) {
         const LineSeg s = seg[k];
         const double bx = s.vx + rx, by = s.vy + ry, bz = s.vz + rz;    // B - P

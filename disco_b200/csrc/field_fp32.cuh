@@ -91,7 +91,7 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
     float ea = ex * ax + ey * ay + ez * az;
     float zr = 1.0f, zi = 0.0f, lx = 0.0f, ly = 0.0f, lz = 0.0f;
     const int nseg = pc.nseg;
-#pragma unroll 2
+#pragma unroll 8
     for (int k = 0; k < nseg; ++k) {
         const LineSegF s = seg[k];
         const float bx = s.vx - Px, by = s.vy - Py, bz = s.vz - Pz;

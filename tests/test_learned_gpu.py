@@ -141,33 +141,43 @@ def test_network_gains_over_truncation_and_is_faster_than_exact():
     assert r["total_max"] < 0.25 * r["truncation_max"], r
     assert r["total_max"] < 1e-3, r
     assert r["loop_rel_rms"] < 0.2, r
-    # speed: the network against the exact far-shell sum on the same pairs
+    # speed: the network against the exact far-shell sum on the same pairs; each
+    # figure is the best of a few calls, so that a host-side stall between the
+    # two events of one call (an allocator release, say) does not count
     big = torch.tensor(rng.uniform(-L / 2, L / 2, size=(3, 32768)), dtype=torch.float64, device="cuda")
     u = torch.zeros_like(big)
-    Ln.far_apply(m, norm, big, held, box, u=u)
-    torch.cuda.synchronize()
-    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    e0.record()
-    Ln.far_apply(m, norm, big, held, box, u=u)
-    e1.record()
+
+    def best_ms(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
     p = B.Plan(held, box, images=4, nu=0.34, image_min=2)
-    e2.record()
-    e3 = torch.cuda.Event(enable_timing=True)
-    p.execute(big, u)
-    e3.record()
-    p.sync()
-    t_net, t_exact = e0.elapsed_time(e1), e2.elapsed_time(e3)
+    pd = B.Plan(Ln.dipole_loops(held), box, images=4, nu=0.34, image_min=2)
+
+    def exact():
+        p.execute(big, u)
+        p.sync()
+
+    def dipole():
+        pd.execute(big, u)
+        pd.sync()
+
+    t_net = best_ms(lambda: Ln.far_apply(m, norm, big, held, box, u=u), 5)
+    t_exact = best_ms(exact, 2)
     assert t_net * 20 < t_exact, (t_net, t_exact)
     # the far-field dipole (one Kroupa loopon of area A per loop, cf. the far-field
     # test of Code/tests/test_barnett.cpp) is more accurate but 702 loopon
     # evaluations per (atom, loop): the network is faster
-    pd = B.Plan(Ln.dipole_loops(held), box, images=4, nu=0.34, image_min=2)
-    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e4.record()
-    pd.execute(big, u)
-    e5.record()
-    pd.sync()
-    t_dipole = e4.elapsed_time(e5)
+    t_dipole = best_ms(dipole, 3)
     assert t_net * 3 < t_dipole, (t_net, t_dipole)
     assert r["dipole_max"] < r["truncation_max"], r
 

@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--epochs", type=int, default=32, help="learned: training epochs over 2^22 samples")
     p.add_argument("--no-fp64", action="store_true", help="learned: skip the plain FP64 comparison run")
     p.add_argument("--no-output", action="store_true", help="skip the output-writer measurement")
+    p.add_argument("--no-forms", action="store_true",
+                   help="default workload: skip the fp32c, learned and bcc_prismatic keys")
     return p.parse_args()
 
 
@@ -88,8 +90,12 @@ class L2Flush:
             self.buf.fill_(1)
 
     def note(self, input_bytes):
-        return (f"L2 flushed between timed steps (inputs {input_bytes / 1e6:.0f} MB < L2)" if self.on else
-                f"inputs larger than L2 ({input_bytes / 1e6:.0f} MB)")
+        return l2_note(input_bytes)
+
+
+def l2_note(input_bytes):
+    return (f"L2 flushed between timed steps (inputs {input_bytes / 1e6:.0f} MB < L2)" if input_bytes < L2_BYTES
+            else f"inputs larger than L2 ({input_bytes / 1e6:.0f} MB)")
 
 
 def timed_steps(torch, step, steps, stream, flush):
@@ -138,12 +144,21 @@ def max_over_ranks(value, world, device="cuda"):
     return float(t.item())
 
 
-def build_workload(name, images=None):
+def build_workload(name, images=None, geom=None):
     from disco_b200 import workloads as W
-    w = W.FULL[name]()
+    w = W.FULL[name](geom=geom)
     if images is not None:
         w.images = images
     return w
+
+
+def arm_config(args, w, precision, n_segments, n_loopons, image_min=0):
+    """The `config` of a bench line, the same for both arms."""
+    W_ = 2 * w.images + 1
+    inner = 2 * image_min - 1 if image_min > 0 else 0
+    return {"workload": args.config, "atoms": w.n, "loops": len(w.loops), "segments": int(n_segments),
+            "loopons": int(n_loopons), "images": W_ ** 3 - inner ** 3, "nu": w.nu, "method": w.method,
+            "precision": precision, "l2": l2_note(48 * w.n), "parallelism": f"replicas x{args.gpus}"}
 
 
 def flop_per_eval(w):
@@ -245,6 +260,27 @@ def fp32_peak_tflops(torch):
         torch.backends.cuda.matmul.allow_tf32 = old
 
 
+def pipe_peak_tflops(torch, clk, fp64=True):
+    """Peak of the CUDA-core FMA pipe a field kernel runs on: SMs x FMA lanes
+    per SM per clock (64 FP64, 128 FP32 on B200) x 2 flop x the median SM
+    clock sampled during the timed region (clocks.max.sm without samples).
+    Returns (TFLOP/s, how it was derived)."""
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz, src = (clk or {}).get("sm_mhz"), "median SM clock sampled in the timed region"
+    if not mhz:
+        try:
+            out = subprocess.run(["nvidia-smi", "-i", str(torch.cuda.current_device()),
+                                  "--query-gpu=clocks.max.sm", "--format=csv,noheader,nounits"],
+                                 capture_output=True, text=True, timeout=20).stdout
+            mhz, src = float(out.strip().splitlines()[0]), "clocks.max.sm (no samples)"
+        except Exception:
+            mhz, src = 1965.0, "1965 MHz nominal (no clock reading)"
+    lanes = 64 if fp64 else 128
+    tf = sms * lanes * 2 * mhz * 1e6 / 1e12
+    return tf, (f"{'FP64' if fp64 else 'FP32'} FMA pipe: {sms} SMs x {lanes} lanes x 2 flop x "
+                f"{mhz:.0f} MHz ({src})")
+
+
 def traffic_from_profiles(kernel_key):
     """DRAM bytes per launch from the committed ncu summary, if any."""
     path = os.path.join(ROOT, "profiles", f"{kernel_key}.md")
@@ -259,6 +295,65 @@ def traffic_from_profiles(kernel_key):
     return None
 
 
+class quiet_stdout:
+    """Sends file descriptor 1 to /dev/null for the duration (the reference's
+    backends print progress lines with std::cout; the bench prints one JSON
+    line)."""
+
+    def __enter__(self):
+        import ctypes
+        sys.stdout.flush()
+        self.libc = ctypes.CDLL(None)
+        self.libc.fflush(None)
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        self.libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+        return False
+
+
+def reference_gpu(w, x, y, z, ours_u=None, reps=3):
+    """The reference's own CUDA backend (Code/backend_cuda.cu, built for
+    sm_100a in oracle/_ref) on the same GPU and atoms: kroupaGPU per call
+    (allocation, upload, one launch and one device wait per loop, download,
+    free: its host-buffer drop-in, like this library's e2e) and its own
+    kernel time (host clock around the per-loop launches and waits), FP64 and
+    --fp32, best of `reps`.  Images +-1 and nu 0.35 are fixed there; the
+    cost does not depend on nu.  max_abs_du: against this library's FP64
+    result on the same atoms when given (ours_u, shape (3, n))."""
+    import oracle as O
+    if not O.have_ref_cuda():
+        return {"unavailable": "the reference's CUDA backend is not built here (oracle/_ref)"}
+    if w.images != 1:
+        return {"unavailable": "the reference's kernels fix the images at +-1"}
+    n = len(x)
+    evals = w.evals_per_atom() * n
+    out = {"what": "kroupaGPU of Code/backend_cuda.cu built for sm_100a (nvcc -O3, its Makefile flags)",
+           "atoms": n, "images": 27, "nu": 0.35}
+    with quiet_stdout():
+        O.ref_displace_gpu(x[:256], y[:256], z[:256], w.loops, w.box)          # context, module load
+    for fp32 in (False, True):
+        best_call, best_k, u = 1e30, 1e30, None
+        for _ in range(reps):
+            with quiet_stdout():
+                t0 = time.perf_counter()
+                u, t = O.ref_displace_gpu(x, y, z, w.loops, w.box, fp32=fp32)
+                call = time.perf_counter() - t0
+            best_call, best_k = min(best_call, call), min(best_k, float(t[1]))
+        r = {"call_s": best_call, "kernels_s": best_k, "atoms_per_s": n / best_call,
+             "kernel_atoms_per_s": n / best_k, "kernel_evals_per_s": evals / best_k}
+        if ours_u is not None and not fp32:
+            r["max_abs_du_vs_ours_fp64"] = float(max(np.abs(u[k] - ours_u[k]).max() for k in range(3)))
+        out["fp32" if fp32 else "fp64"] = r
+    return out
+
+
 def cpu_baseline(w, seconds, use_reference):
     """Atoms/s of a CPU implementation on a seeded atom sample (all threads)."""
     import oracle as O
@@ -270,7 +365,8 @@ def cpu_baseline(w, seconds, use_reference):
         x, y, z = w.x[idx], w.y[idx], w.z[idx]
         t0 = time.perf_counter()
         if ref_ok:
-            u = O.ref_displace(x, y, z, w.loops, w.box)
+            with quiet_stdout():
+                u = O.ref_displace(x, y, z, w.loops, w.box)
         else:
             u = O.displace(x, y, z, w.loops, w.box, images=w.images, nu=w.nu, threads=threads)
         return time.perf_counter() - t0, u
@@ -304,7 +400,7 @@ def run_reference_batch(args):
     from disco_b200 import workloads as W
     import oracle as O
     threads = os.cpu_count() or 1
-    batch = W.batch(nsamples=args.samples)
+    batch = W.batch(nsamples=args.samples, geom=O.RefGeometry if O.have_ref() else None)
     n = sum(w.n for w in batch)
     evals = sum(w.n * w.evals_per_atom() for w in batch)
     rng = np.random.default_rng(99)
@@ -344,9 +440,14 @@ def run_reference(args):
         return
     if args.config == "batch":
         return run_reference_batch(args)
-    # the learned workload's reference is the exact sum over all 729 images (+-4)
-    w = build_workload("fcc_random", 4) if args.config == "learned" else build_workload(args.config, args.images)
     import oracle as O
+    # inputs built by the reference's own geometry code where it is compiled
+    # here (lattice, mid-plane snap, loop class, polylines, loopon grids), so
+    # that this arm runs nothing of this library
+    geom = O.RefGeometry if O.have_ref() else None
+    # the learned workload's reference is the exact sum over all 729 images (+-4)
+    w = build_workload("fcc_random", 4, geom) if args.config == "learned" else \
+        build_workload(args.config, args.images, geom)
     threads = os.cpu_count() or 1
     ref_ok = w.images == 1 and O.have_ref()
     rng = np.random.default_rng(99)
@@ -354,7 +455,8 @@ def run_reference(args):
     def run(idx):
         t0 = time.perf_counter()
         if ref_ok:
-            O.ref_displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box)
+            with quiet_stdout():
+                O.ref_displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box)
         else:
             O.displace(w.x[idx], w.y[idx], w.z[idx], w.loops, w.box, images=w.images, nu=w.nu,
                        threads=threads)
@@ -379,14 +481,25 @@ def run_reference(args):
     T = sum(times)
     value = k * args.steps / T
     kind = "reference" if ref_ok else "port"
-    sample = f"{k} seeded random atoms of {w.n} per step, all loops and images"
+    sample = (f"{k} seeded random atoms of {w.n} per step, all loops and images; inputs from "
+              f"{'the reference geometry code (oracle/_ref)' if geom else 'this library geometry'}")
+    nseg = sum(len(lp.vx) for lp in w.loops if lp.line)
+    nlp = sum(len(lp.x) for lp in w.loops if not lp.line)
+    if args.config == "learned":
+        cfg = {"workload": "fcc_random_learned", "atoms": w.n, "loops": len(w.loops), "segments": nseg,
+               "images": 729, "nu": w.nu}
+    else:
+        cfg = arm_config(args, w, args.precision, nseg, nlp)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "atoms/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * T / args.steps * (w.n / k), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.config, "atoms": w.n, "loops": len(w.loops),
-                   "images": (2 * w.images + 1) ** 3, "nu": w.nu, "method": w.method},
+        "config": cfg,
+        "extrapolated": {"sampled_atoms_per_step": k, "atoms": w.n, "timed_seconds": T,
+                         "note": "each step times a seeded sample of the workload's atoms with all loops "
+                                 "and images; value is the sample's atoms/s and ms_per_step that rate "
+                                 "scaled to every atom (per-atom cost is uniform)"},
         "cpu_baseline": {"value": value, "unit": "atoms/s", "cores": threads, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -449,6 +562,94 @@ def write_output(w, pos, u, stream):
             "atoms": n, "bytes": int(nbytes.value), "ms": e0.elapsed_time(e1), "wall_ms": 1e3 * wall,
             "atoms_per_s": n / (e0.elapsed_time(e1) * 1e-3), "bytes_match_oracle_first_atoms": m if ok else 0,
             "cpu_oracle_atoms_per_s_1_thread": cpu_rate}
+
+
+def fp32c_form(args, w, pos, u64, idx, uref):
+    """The FP32 compensated form on the default workload's atoms: device-resident
+    step time, roofline against the FP32 FMA pipe, max and RMS |du| against the
+    plain FP64 result on every atom and against the oracle on the parity
+    sample (idx, uref)."""
+    import torch
+    from disco_b200 import backend as B
+    from disco_b200 import _capi as C
+    stream = torch.cuda.current_stream()
+    n = w.n
+    plan = B.Plan(w.loops, w.box, precision=C.DISCO_FP32C, images=w.images, nu=w.nu, max_atoms=n)
+    st = plan.stats()
+    u = torch.zeros_like(pos)
+    for _ in range(args.warmup):
+        plan.execute(pos, u)
+    plan.sync(stream.cuda_stream)
+    flush = L2Flush(torch, 48 * n)
+    clocks = Clocks(torch.cuda.current_device())
+    torch.cuda.synchronize()
+    clocks.start()
+    el = timed_steps(torch, lambda: plan.execute(pos, u), args.steps, stream, flush)
+    clk = clocks.stop()
+    plan.sync(stream.cuda_stream)
+    per = el / args.steps
+    u.zero_()
+    plan.execute(pos, u)
+    plan.sync(stream.cuda_stream)
+    plan.close()
+    uf = u.cpu().numpy()
+    del u
+    d = uf - u64
+    evals = st["evals_per_atom"] * n
+    achieved = evals * W_LINE / per / 1e12
+    peak, src = pipe_peak_tflops(torch, clk, fp64=False)
+    gemm = fp32_peak_tflops(torch)
+    out = {"value": n / per, "unit": "atoms/s", "ms_per_step": 1e3 * per, "steps": args.steps,
+           "speedup_vs_fp64": None, "evals_per_s": evals / per,
+           "max_abs_du": float(np.abs(d).max()), "rms_du": float(np.sqrt(np.mean(d * d))),
+           "against": "plain FP64 result (this run, every atom; itself within 1e-9 A of the oracle)",
+           "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak, "peak_source": src, "peak_gemm": gemm,
+                        "frac_of_gemm": achieved / gemm, "flop_per_eval": W_LINE, "evals_per_launch": evals},
+           "clocks": clk, "gpu_launches": 2 * args.steps}
+    if idx is not None:
+        out["max_abs_du_vs_oracle_sample"] = float(np.abs(uf[:, idx] - np.stack(uref)).max())
+        out["oracle_sample_atoms"] = int(len(idx))
+    return out
+
+
+def north_star_forms(args, w, pos, u64, idx, uref):
+    """The forms the target names beside the plain FP64 path, each timed on its
+    own (CUDA events, its own clock samples) after the headline measurement:
+      fp32c          the FP32 compensated form on the same atoms;
+      learned        images +-4 with the network's far shells: speed-up over the
+                     plain FP64 path on the same workload, max/RMS |du| on every
+                     atom, per-loop fallbacks, training time;
+      bcc_prismatic  the matter step + loopon field + epilogue: step time,
+                     bit-exact atom sets, compaction rate."""
+    import argparse as ap
+    import torch
+    sub = ap.Namespace(**{**vars(args), "steps": 3, "warmup": 1, "e2e_steps": 1, "no_cpu": True,
+                          "no_output": True, "image_split": 0, "images": None, "retrain": False,
+                          "no_fp64": False, "precision": "fp64"})
+    out = {}
+    f = fp32c_form(sub, w, pos, u64, idx, uref)
+    out["fp32c"] = f
+    torch.cuda.empty_cache()
+    ln = run_learned(sub, embedded=(w, pos))
+    L = ln["learned"]
+    out["learned"] = {
+        "value": ln["value"], "unit": "atoms/s", "ms_per_step": ln["ms_per_step"], "steps": ln["steps"],
+        "speedup_vs_fp64": L["speedup_vs_fp64"], "fp64_ms_per_step": (ln["fp64_exact"] or {}).get("ms_per_step"),
+        "max_abs_du": (L["accuracy"] or {}).get("max_abs_du"), "rms_du": (L["accuracy"] or {}).get("rms_du"),
+        "truncated_max_abs_du": (L["accuracy"] or {}).get("truncated_max_abs_du"),
+        "against": (L["accuracy"] or {}).get("against"), "n_fallback": L["n_fallback"],
+        "check_max": L["check_max"], "phase_seconds": L["phase_seconds"],
+        "training_seconds": L["training"].get("train_seconds"), "training": L["training"],
+        "config": {k: ln["config"][k] for k in ("images", "near_images", "far_images", "near", "far", "check")},
+        "roofline_near_shell": ln["roofline"], "clocks": ln["clocks"], "gpu_launches": ln["gpu_launches"]}
+    torch.cuda.empty_cache()
+    pr = run_prismatic(sub, embedded=True)
+    out["bcc_prismatic"] = {
+        "value": pr["value"], "unit": "atoms/s", "ms_per_step": pr["ms_per_step"], "steps": pr["steps"],
+        "config": pr["config"], "parity": pr["parity"], "compaction": pr["compaction"],
+        "roofline_loopon_field": pr["roofline"], "clocks": pr["clocks"], "gpu_launches": pr["gpu_launches"]}
+    return out
 
 
 def run_ours(args):
@@ -523,17 +724,20 @@ def run_ours(args):
            "h2d_bytes_per_step": 6 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n, "steps": e2e_steps}
 
     if rank == 0:
-        peak = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else fp32_peak_tflops(torch)
+        fp64 = prec == C.DISCO_FP64
+        gemm = fp64_peak_tflops(torch) if fp64 else fp32_peak_tflops(torch)
+        peak, peak_src = pipe_peak_tflops(torch, clk, fp64)
         flops = evals_atom * n * flop_per_eval(w)
         achieved = flops / per_launch / 1e12
         key = f"{'line' if w.method == 'line' else 'loopon'}_{args.precision}_{args.config}"
         traffic = traffic_from_profiles(key)
-        roof = {"bound": "fp64" if prec == C.DISCO_FP64 else "fp32", "achieved": achieved,
-                "peak": peak, "unit": "TFLOP/s", "frac": (achieved / peak) if peak else None,
-                "traffic": traffic,
-                "peak_source": ("measured here: torch DGEMM 8192^3 best of 5" if prec == C.DISCO_FP64 else
-                                "measured here: torch SGEMM 8192^3 without TF32, best of 5") +
-                               " (MEASURED_PEAKS.json has no FP64 or FP32 CUDA-core figure)",
+        roof = {"bound": "fp64" if fp64 else "fp32", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                "peak_source": peak_src + "; MEASURED_PEAKS.json has no FP64 or FP32 CUDA-core figure",
+                "peak_gemm": gemm, "frac_of_gemm": achieved / gemm if gemm else None,
+                "peak_gemm_source": ("torch DGEMM 8192^3, best of 5: it runs on the FP64 tensor-core path, "
+                                     "not on the DFMA pipe this kernel uses") if fp64 else
+                                    "torch SGEMM 8192^3 without TF32, best of 5",
                 "flop_per_eval": flop_per_eval(w), "evals_per_launch": evals_atom * n}
         cpu = None
         parity = None
@@ -542,19 +746,30 @@ def run_ours(args):
             du = np.abs(u1[:, idx] - np.stack(ucpu)).max()
             parity = {"max_abs_du": float(du), "atoms": int(len(idx)), "against": "oracle"}
             cpu.pop("seconds", None)
+        refgpu = None
+        if world == 1 and args.config == "quadrupole" and fp64:
+            p35 = B.Plan(w.loops, w.box, precision=C.DISCO_FP64, images=1, nu=0.35, max_atoms=n)
+            u35 = torch.zeros_like(pos)
+            p35.execute(pos, u35)
+            p35.sync(stream.cuda_stream)
+            p35.close()
+            refgpu = reference_gpu(w, w.x, w.y, w.z, ours_u=u35.cpu().numpy())
+            del u35
+            refgpu["ours"] = {"kernel_atoms_per_s": value, "e2e_atoms_per_s": e2e["value"],
+                              "note": "this library on the same atoms (nu 0.29: same operation count)"}
+        forms = {}
+        if world == 1 and not args.no_forms and args.config == "fcc_random" and fp64:
+            forms = north_star_forms(args, w, pos, u1, idx if parity else None, ucpu if parity else None)
         line = {
             "metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_launch,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if prec == C.DISCO_FP64 else "f32c", "data": "synthetic",
-            "config": {"workload": args.config, "atoms": n, "loops": len(w.loops),
-                       "segments": st["n_segments"], "loopons": st["n_loopons"],
-                       "images": st["n_images"], "nu": w.nu, "method": w.method,
-                       "precision": args.precision, "l2": flush.note(48 * n),
-                       "parallelism": f"replicas x{world}"},
+            "config": arm_config(args, w, args.precision, st["n_segments"], st["n_loopons"]),
             "evals_per_s": evals_atom * n * world * args.steps / elapsed,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps, "parity": parity, "output": output,
+            **({"reference_gpu": refgpu} if refgpu else {}), **forms,
         }
         print(json.dumps(line), flush=True)
     plan.close()
@@ -695,24 +910,33 @@ def run_batch(args):
         dist.destroy_process_group()
 
 
-def run_learned(args):
+def run_learned(args, embedded=None):
     """Learned form on the fcc_random geometry with images +-4 (729 images):
     exact near images +-1 (27, FP32 compensated), the network's far shells
     2 <= max|n| <= 4 (702 images), the exact FP64 far-shell sum re-checked on a
     1 % stratified random atom subsample every step with per-loop fallback.
     The plain FP64 path on the same workload (all 729 images exact) is timed
-    once and is the reference for the learned result on every atom."""
+    once and is the reference for the learned result on every atom.
+    embedded = (fcc_random workload, its positions on the device): one GPU,
+    returns the line instead of printing it."""
     import torch
     from disco_b200 import backend as B
     from disco_b200 import _capi as C
     from disco_b200 import learned as Ln
     rank, world, local = dist_env()
+    if embedded is not None:
+        rank, world = 0, 1
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
-    w = build_workload("fcc_random", 4)
+    if embedded is not None:
+        import copy
+        w = copy.copy(embedded[0])
+        w.images = 4
+    else:
+        w = build_workload("fcc_random", 4)
     n = w.n
     log = (lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None
     path = os.environ.get("DISCO_B200_FAR_NET",
@@ -724,7 +948,8 @@ def run_learned(args):
     m, norm, info = Ln.cached_or_train(path if rank == 0 else None, log=log, nloops=4096, atoms=1024, seed=5,
                                        nu=w.nu, epochs=args.epochs)
     stream = torch.cuda.current_stream()
-    pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
+    pos = embedded[1] if embedded is not None else \
+        torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
     u = torch.zeros_like(pos)
 
     def barrier():
@@ -800,7 +1025,8 @@ def run_learned(args):
         segs = sum(len(lp.vx) for lp in w.loops)
         near_evals = segs * 27 * n
         t_near = statistics.median(r["t_near"] for r in reps)
-        peak = fp32_peak_tflops(torch)
+        peak, peak_src = pipe_peak_tflops(torch, clk, fp64=False)
+        gemm = fp32_peak_tflops(torch)
         achieved = near_evals * W_LINE / t_near / 1e12
         cpu = None
         if not args.no_cpu:
@@ -827,11 +1053,14 @@ def run_learned(args):
             "fp64_exact": fp64,
             "roofline": {"bound": "fp32", "kernel": "near-shell FP32 line kernel", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                         "peak_source": "measured here: torch SGEMM 8192^3 without TF32, best of 5",
+                         "peak_source": peak_src, "peak_gemm": gemm, "frac_of_gemm": achieved / gemm,
+                         "peak_gemm_source": "torch SGEMM 8192^3 without TF32, best of 5",
                          "flop_per_eval": W_LINE, "evals_per_launch": near_evals},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": sum(r["launches"] for r in reps),
         }
+        if embedded is not None:
+            return line
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
@@ -840,11 +1069,14 @@ def run_learned(args):
 
 def compaction_rate(lib, C, torch, stream):
     """The matter step alone (disco_b200_prismatic_noalloc: slab membership,
-    stable compaction, new-index map, copies) on the largest box it takes,
-    BCC 128^3 = 4 194 304 atoms with 16 loops of the bcc_prismatic distribution:
-    achieved GB/s of the algorithmic bytes (76 B per atom: positions read twice,
-    survivors written, 4 B index) against the measured HBM peak.  The call
-    includes two small device-to-host reads of the counts (its host syncs)."""
+    stable compaction, new-index map, slab entries, copies) on the largest box
+    it takes, BCC 128^3 = 4 194 304 atoms with 16 loops of the bcc_prismatic
+    distribution: achieved GB/s of the algorithmic bytes (52 B per atom:
+    positions read once, survivors written, 4 B new index; the slab entries
+    and copies add a few hundred KB) against the measured HBM peak.  Timed per
+    call with CUDA events around the whole call, which ends with one
+    device-to-host read of the totals (its only host wait); the single-pass
+    kernel alone is timed too."""
     import ctypes
     from disco_b200 import workloads as W
     w = W.bcc_prismatic(cells=128)
@@ -872,32 +1104,36 @@ def compaction_rate(lib, C, torch, stream):
     for _ in range(3):
         call()
     torch.cuda.synchronize()
-    reps = 10
-    flush = L2Flush(torch, 0)                     # always: 100 MB of positions, read twice
+    reps = 20
+    flush = L2Flush(torch, 0)                     # always: 100 MB of positions < L2
     t = timed_steps(torch, call, reps, stream, flush) / reps
     pk = measured_peaks()
     peak = pk["hbm_gbs"] if pk else 6650.0
-    gbs = 76.0 * n / t / 1e9
+    gbs = 52.0 * n / t / 1e9
     return {"atoms": n, "survivors": int(counts[0]), "slab_atoms": int(counts[1]), "copies": int(counts[2]),
-            "ms": 1e3 * t, "atoms_per_s": n / t, "algorithmic_bytes": 76 * n, "achieved_gbs": gbs,
+            "ms": 1e3 * t, "atoms_per_s": n / t, "algorithmic_bytes": 52 * n, "achieved_gbs": gbs,
             "peak_gbs": peak, "frac": gbs / peak, "l2": "flushed before each timed call",
+            "timed": "whole call (loop upload, pass, tail, totals read back) with CUDA events",
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk else "fallback 6650 GB/s"}
 
 
-def run_prismatic(args):
+def run_prismatic(args, embedded=False):
     """The bcc_prismatic workload: one step = the prismatic matter step (slab selection, vacancy
     removal, interstitial copies; disco_b200_prismatic_noalloc on device
     arrays), the loopon field of all 16 loops over the surviving atoms (plan),
     and the fused copy/add-u/wrap epilogue (disco_b200_finalize_resident).
     value = input atoms / step time.  Parity: atom sets, order, copies bit-exact
     against the oracle; the field on a seeded survivor sample within 1e-9 A
-    (FP64); the final positions of that sample against the oracle's epilogue."""
+    (FP64); the final positions of that sample against the oracle's epilogue.
+    embedded: one GPU, returns the line instead of printing it."""
     import ctypes
     import torch
     from disco_b200 import backend as B
     from disco_b200 import _capi as C
     from disco_b200 import prismatic as P
     rank, world, local = dist_env()
+    if embedded:
+        rank, world = 0, 1
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
@@ -1010,7 +1246,28 @@ def run_prismatic(args):
             cpu, _, _ = cpu_baseline(w, args.cpu_seconds, use_reference=False)
             cpu.pop("seconds", None)
             cpu["sample"] += "; the matter step is not in the CPU figure (host serial in the reference, ms)"
-        peak = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else fp32_peak_tflops(torch)
+        refgpu = None
+        if not embedded and prec == C.DISCO_FP64:
+            # the loopon field over the survivors, the reference's kernels against ours at its nu
+            p35 = B.Plan(w.loops, w.box, precision=C.DISCO_FP64, images=1, nu=0.35, max_atoms=k)
+            u35 = torch.zeros((3, k), dtype=torch.float64, device="cuda")
+            p35.execute_ptrs(out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), u35[0].data_ptr(),
+                             u35[1].data_ptr(), u35[2].data_ptr(), k, stream.cuda_stream)
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            u35.zero_()
+            f0.record(stream)
+            p35.execute_ptrs(out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), u35[0].data_ptr(),
+                             u35[1].data_ptr(), u35[2].data_ptr(), k, stream.cuda_stream)
+            f1.record(stream)
+            p35.sync(stream.cuda_stream)
+            p35.close()
+            refgpu = reference_gpu(w, o[0, :k].copy(), o[1, :k].copy(), o[2, :k].copy(),
+                                   ours_u=u35.cpu().numpy(), reps=1)
+            refgpu["ours"] = {"kernel_s": f0.elapsed_time(f1) * 1e-3,
+                              "note": "this library's loopon field over the same survivors, nu 0.35"}
+            del u35
+        gemm = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else fp32_peak_tflops(torch)
+        peak, peak_src = pipe_peak_tflops(torch, clk, prec == C.DISCO_FP64)
         achieved = evals * W_LOOPON / per / 1e12
         line = {
             "metric": METRIC, "value": n * world / per, "unit": "atoms/s", "n_gpus": world,
@@ -1025,6 +1282,8 @@ def run_prismatic(args):
             "evals_per_s": evals * world / per,
             "roofline": {"bound": "fp64" if prec == C.DISCO_FP64 else "fp32", "kernel": "loopon field",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": peak_src + " (the step also holds the matter step and epilogue)",
+                         "peak_gemm": gemm, "frac_of_gemm": achieved / gemm,
                          "traffic": None, "flop_per_eval": W_LOOPON, "evals_per_launch": evals},
             "cpu_baseline": cpu,
             "e2e": {"value": n * world * e2e_steps / e2e_t, "unit": "atoms/s",
@@ -1032,7 +1291,11 @@ def run_prismatic(args):
                     "d2h_bytes_per_step": 28 * n + 24 * k + 48 * (k + nc), "steps": e2e_steps},
             "clocks": clk, "gpu_launches": args.steps * 6,     # count, scan, scatter, copies, field, epilogue
             "parity": parity, "compaction": compaction,
+            **({"reference_gpu": refgpu} if refgpu else {}),
         }
+        if embedded:
+            plan.close()
+            return line
         print(json.dumps(line), flush=True)
     plan.close()
     if world > 1:

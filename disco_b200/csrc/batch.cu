@@ -31,6 +31,7 @@ struct SampleDev {
     const Chunk* chunks;
     const LinePiece* pieces64;      // FP32 line form: FP64 pieces for the near-cut pass
     const LineSeg* segs64;
+    const double* raw;              // line method: input vertex triplets
     int32_t nchunks, images, nimg, image_min;
     double Lx, Ly, Lz;
 };
@@ -117,7 +118,7 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
         fa.Lx = sd.Lx; fa.Ly = sd.Ly; fa.Lz = sd.Lz;
         fa.cJ = b.cJ; fa.cK = b.cK; fa.c2 = b.c2;
         fa.near_h = b.near_h; fa.near_r = b.near_r;
-        fa.pieces64 = sd.pieces64; fa.segs64 = sd.segs64;
+        fa.pieces64 = sd.pieces64; fa.segs64 = sd.segs64; fa.raw = sd.raw;
         const unsigned char* st = stage0 + (size_t)buf * b.stage_bytes;
         Policy::template chunk<S>(fa, st, sd.chunks[un.chunk].npieces, split, px, py, pz, acc);
         if (un.last) {
@@ -335,7 +336,8 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
         const int kind = k == 0 ? kLineKind : kLooponKind;
         std::vector<unsigned char> bytes;
         std::vector<SampleDev> sdev(nsamples);
-        std::vector<uint64_t> chunk_off(nsamples, 0), aux_off(nsamples, 0), aux_segs(nsamples, 0);
+        std::vector<uint64_t> chunk_off(nsamples, 0), aux_off(nsamples, 0), aux_segs(nsamples, 0),
+            aux_raw(nsamples, 0);
         std::vector<std::vector<Chunk>> chunks(nsamples);
         std::vector<double> work(nsamples, 0.0);        // evaluations per atom of each sample
         bool any = false;
@@ -365,6 +367,7 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
             chunks[s] = T.chunks;
             aux_off[s] = T.aux_pieces ? base + T.aux_pieces : 0;
             aux_segs[s] = T.aux_segs ? base + T.aux_segs : 0;
+            aux_raw[s] = T.aux_raw ? base + T.aux_raw : 0;
             for (const Chunk& c : T.chunks) max_stage = std::max(max_stage, c.bytes);
             const int inner = sm.image_min > 0 ? 2 * sm.image_min - 1 : 0;
             work[s] = (double)(T.n_segments + T.n_loopons) * (sdev[s].nimg - inner * inner * inner);
@@ -393,6 +396,7 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
             // chunk offsets are relative to the sample's own table
             sdev[s].table = p->d_table[k] + chunk_off[s];
             sdev[s].chunks = d_chunks + chunk_base[s];
+            if (aux_raw[s]) sdev[s].raw = reinterpret_cast<const double*>(p->d_table[k] + aux_raw[s]);
             if (aux_off[s]) {
                 sdev[s].pieces64 = reinterpret_cast<const LinePiece*>(p->d_table[k] + aux_off[s]);
                 sdev[s].segs64 = reinterpret_cast<const LineSeg*>(p->d_table[k] + aux_segs[s]);

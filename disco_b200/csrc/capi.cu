@@ -254,6 +254,8 @@ int disco_b200_plan_execute(disco_plan* p, const disco_atoms* a, void* stream)
         fa.status = p->d_status;
         fa.near_h = (float)p->opt.near_plane;
         fa.near_r = (float)p->opt.near_rim;
+        if (k == 0 && T.aux_raw)
+            fa.raw = reinterpret_cast<const double*>(p->d_table[k] + T.aux_raw);
         if (T.fp32 && k == 0 && T.aux_pieces) {
             fa.pieces64 = reinterpret_cast<const disco::LinePiece*>(p->d_table[k] + T.aux_pieces);
             fa.segs64 = reinterpret_cast<const disco::LineSeg*>(p->d_table[k] + T.aux_segs);

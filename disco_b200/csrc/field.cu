@@ -32,6 +32,15 @@
 
 namespace disco {
 
+// Appends the raw vertex triplets to the table bytes (16-byte aligned).
+void append_raw(HostTable& T, const std::vector<double>& raw)
+{
+    while (T.bytes.size() % 16) T.bytes.push_back(0);
+    T.aux_raw = T.bytes.size();
+    const unsigned char* s = reinterpret_cast<const unsigned char*>(raw.data());
+    T.bytes.insert(T.bytes.end(), s, s + raw.size() * sizeof(double));
+}
+
 int build_table(const disco_loop* loops, int nloops, int kind, int precision, double nu,
                 HostTable& T, std::string& err, uint32_t stage_cap)
 {
@@ -43,6 +52,7 @@ int build_table(const disco_loop* loops, int nloops, int kind, int precision, do
     const double k1 = 1.0 / (8.0 * M_PI * (1.0 - nu));          // Code/kroupa.hpp:38-41
     if (kind == kLineKind) {
         PieceList<LinePiece, LineSeg> L;
+        std::vector<double> raw;
         for (int l = 0; l < nloops; ++l) {
             const disco_loop& lp = loops[l];
             if (!lp.line) continue;
@@ -58,12 +68,13 @@ int build_table(const disco_loop* loops, int nloops, int kind, int precision, do
                 const int k1e = std::min(nv, k0 + kMaxLinePiece);
                 LinePiece p;
                 std::vector<LineSeg> recs;
-                make_line_piece(lp, k0, k1e, bx, by, bz, k1, p, recs);
+                make_line_piece(lp, k0, k1e, bx, by, bz, k1, p, recs, raw);
                 L.pieces.push_back(p);
                 L.recs.push_back(std::move(recs));
             }
         }
         pack_chunks(L, T, stage_cap);
+        if (!T.chunks.empty()) append_raw(T, raw);
     } else {
         PieceList<LooponPiece, LooponRec> L;
         for (int l = 0; l < nloops; ++l) {

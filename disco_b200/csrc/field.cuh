@@ -29,8 +29,12 @@ struct alignas(16) LinePiece {
     double bx, by, bz;   // Burgers vector (phys.b * m)
     double rho;          // largest |vertex - apex| over the piece's vertices
     double lmax;         // longest segment of the piece
+    double nx, ny, nz;   // unit normal of the loop's mean plane (area vector)
+    double hband;        // |n.(apex - P)| <= hband: the solid angle is taken per triangle
     int32_t nseg;        // segments of this piece
     int32_t rec;         // first segment record, index into the chunk's records
+    int32_t raw;         // first of the piece's nseg + 1 input vertices in the raw array
+    int32_t pad;
 };
 struct alignas(16) LineSeg {
     double vx, vy, vz;   // end vertex B of segment A -> B, minus the apex
@@ -40,7 +44,7 @@ struct alignas(16) LineSeg {
     double nx, ny, nz;   // (A - apex) x (B - apex)
     double pad;
 };
-static_assert(sizeof(LinePiece) == 96 && sizeof(LineSeg) == 112, "line table layout");
+static_assert(sizeof(LinePiece) == 144 && sizeof(LineSeg) == 112, "line table layout");
 
 // ---- FP64 loopon method (Code/kroupa.hpp:52-73) ---------------------------------
 struct alignas(16) LooponPiece {
@@ -126,6 +130,9 @@ struct FieldArgs {
     const LinePiece* pieces64;
     const LineSeg* segs64;
     float near_h, near_r;
+    // line method: the loops' input vertices (x, y, z triplets), read only for
+    // an atom on or within hband of a loop's plane
+    const double* raw;
 };
 
 // Host-side table: bytes + chunk list, built once per plan.
@@ -141,7 +148,12 @@ struct HostTable {
     // FP32 line tables: byte offsets of the flat FP64 pieces and segments
     // appended after the chunks (0 when absent)
     uint64_t aux_pieces = 0, aux_segs = 0;
+    // line tables: byte offset of the raw vertex triplets (0 when absent)
+    uint64_t aux_raw = 0;
 };
+
+// Appends a line table's raw vertex triplets after its chunks (sets aux_raw).
+void append_raw(HostTable& T, const std::vector<double>& raw);
 
 // Builds the table of the loops of one kind (kLineKind: loops with line != 0,
 // kLooponKind: the others); returns DISCO_OK or an error code.

@@ -149,18 +149,64 @@ __device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, doub
     }
 }
 
+// Solid angle of a piece's fan seen from P as Code/barnett.hpp:56-72 computes
+// it: per triangle (apex, A, B), 2 atan2(num, den) with num = r1.(a x b),
+// den = l1 la lb + (r1.a) lb + (r1.b) la + (a.b) l1, from r1 = apex - P,
+// a = A - P, b = B - P formed from the input vertices, every operation in the
+// source's order and rounded on its own (no contraction).  For an atom on the
+// loop's plane inside the contour, num is a rounding residue (or a signed
+// zero) and its sign is the branch that puts the atom on one side of the cut
+// (Omega = +-2 pi); for an atom on a fan edge or at the apex the per-triangle
+// arguments are residues too.  Evaluating the reference's expressions
+// operation for operation reproduces its choice in every such case.
+static __device__ __noinline__ double fan_solid_angle_ref(const double* __restrict__ v, int nseg, double cx, double cy,
+                                                   double cz, double px, double py, double pz)
+{
+    const double r1x = __dsub_rn(cx, px), r1y = __dsub_rn(cy, py), r1z = __dsub_rn(cz, pz);
+    const double l1 = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(r1x, r1x), __dmul_rn(r1y, r1y)),
+                                           __dmul_rn(r1z, r1z)));
+    double ax = __dsub_rn(__ldg(v), px), ay = __dsub_rn(__ldg(v + 1), py), az = __dsub_rn(__ldg(v + 2), pz);
+    double la = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay)), __dmul_rn(az, az)));
+    double omega = 0.0;
+    for (int k = 1; k <= nseg; ++k) {
+        const double bx = __dsub_rn(__ldg(v + 3 * k), px), by = __dsub_rn(__ldg(v + 3 * k + 1), py),
+                     bz = __dsub_rn(__ldg(v + 3 * k + 2), pz);
+        const double lb = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz)));
+        const double cxx = __dsub_rn(__dmul_rn(ay, bz), __dmul_rn(az, by));
+        const double cyy = __dsub_rn(__dmul_rn(az, bx), __dmul_rn(ax, bz));
+        const double czz = __dsub_rn(__dmul_rn(ax, by), __dmul_rn(ay, bx));
+        const double num = __dadd_rn(__dadd_rn(__dmul_rn(r1x, cxx), __dmul_rn(r1y, cyy)), __dmul_rn(r1z, czz));
+        const double ra = __dadd_rn(__dadd_rn(__dmul_rn(r1x, ax), __dmul_rn(r1y, ay)), __dmul_rn(r1z, az));
+        const double rb = __dadd_rn(__dadd_rn(__dmul_rn(r1x, bx), __dmul_rn(r1y, by)), __dmul_rn(r1z, bz));
+        const double ab = __dadd_rn(__dadd_rn(__dmul_rn(ax, bx), __dmul_rn(ay, by)), __dmul_rn(az, bz));
+        const double den = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(l1, la), lb), __dmul_rn(ra, lb)),
+                                               __dmul_rn(rb, la)), __dmul_rn(ab, l1));
+        omega = __dadd_rn(omega, __dmul_rn(2.0, atan2(num, den)));
+        ax = bx; ay = by; az = bz; la = lb;
+    }
+    return omega;
+}
+
 // Field at P (an atom moved by minus an image shift) of one line piece.
 // Follows Code/barnett.hpp:55-106 term by term (see field.cu's header for the
 // reformulations); adds b Omega/(4 pi) + the line terms to (ux, uy, uz).
 // Vertices are stored relative to the apex; r = apex - P.  For every segment,
 // RA + RB >= 2 (l1 - rho) with l1 = |apex - P| and rho the piece's largest
 // vertex radius, so t = L/(RA+RB) <= lmax / (2 (l1 - rho)).
+// For an atom within hband of the loop's plane (a little more than the
+// plane's own rounding) the solid angle is left out and `plane` is set: the
+// caller adds it from fan_solid_angle_ref (line_piece_plane) in a second pass,
+// since on the plane the running product's sign is a rounding residue of
+// other operations than the reference's.  Outside the band the product's
+// argument is at least about pi hband / rho away from the branch cut, far
+// above its rounding.
 __device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineSeg* seg,
                                                 double Px, double Py, double Pz, double cJK,
-                                                double& ux, double& uy, double& uz)
+                                                double& ux, double& uy, double& uz, bool& plane)
 {
     // unit vector from P to the fan apex
     const double rx = pc.cx - Px, ry = pc.cy - Py, rz = pc.cz - Pz;
+    const bool on_plane = fabs(pc.nx * rx + pc.ny * ry + pc.nz * rz) <= pc.hband;
     const double l1sq = rx * rx + ry * ry + rz * rz;
     const double il1 = rsqrt_nr(l1sq);
     const double ex = rx * il1, ey = ry * il1, ez = rz * il1;
@@ -176,10 +222,25 @@ __device__ __forceinline__ void line_piece_fp64(const LinePiece& pc, const LineS
     case 1:  line_segments<8>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJK, zr, zi, lx, ly, lz); break;
     default: line_segments<0>(seg, pc.nseg, rx, ry, rz, ex, ey, ez, ax, ay, az, cJK, zr, zi, lx, ly, lz); break;
     }
-    const double f = atan2(zi, zr) * (1.0 / 6.283185307179586476925286766559);   // Omega / (4 pi)
+    double f = atan2(zi, zr) * (1.0 / 6.283185307179586476925286766559);   // Omega / (4 pi)
+    if (on_plane) { f = 0.0; plane = true; }
     ux += pc.bx * f + lx;
     uy += pc.by * f + ly;
     uz += pc.bz * f + lz;
+}
+
+// The solid-angle term b Omega/(4 pi) of one line piece for an atom in its
+// plane band (the part line_piece_fp64 leaves out there); nothing otherwise.
+__device__ __forceinline__ void line_piece_plane(const LinePiece& pc, const double* raw, double Px, double Py,
+                                                 double Pz, double& ux, double& uy, double& uz)
+{
+    const double rx = pc.cx - Px, ry = pc.cy - Py, rz = pc.cz - Pz;
+    if (!(fabs(pc.nx * rx + pc.ny * ry + pc.nz * rz) <= pc.hband)) return;
+    const double f = fan_solid_angle_ref(raw + 3 * (size_t)pc.raw, pc.nseg, pc.cx, pc.cy, pc.cz, Px, Py, Pz) *
+                     (1.0 / 12.566370614359172953850573533118);                 // Omega / (4 pi)
+    ux += pc.bx * f;
+    uy += pc.by * f;
+    uz += pc.bz * f;
 }
 
 // Field at P (atom - reference point - image shift) of one loopon piece:
@@ -238,12 +299,23 @@ struct LineFp64 {
         const LinePiece* pieces = reinterpret_cast<const LinePiece*>(st);
         const LineSeg* recs = reinterpret_cast<const LineSeg*>(st + (size_t)npieces * sizeof(LinePiece));
         const double cJK = a.cJ / a.cK;
+        bool plane = false;
         for (int p = 0; p < npieces; ++p) {
             const LinePiece& pc = pieces[p];
             for (int img = split; img < a.nimg; img += S) {
                 double sx, sy, sz;
                 if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
-                line_piece_fp64(pc, recs + pc.rec, px - sx, py - sy, pz - sz, cJK, acc.x, acc.y, acc.z);
+                line_piece_fp64(pc, recs + pc.rec, px - sx, py - sy, pz - sz, cJK, acc.x, acc.y, acc.z, plane);
+            }
+        }
+        if (plane) {                        // an atom in a loop's plane band: the reference's solid angle
+            for (int p = 0; p < npieces; ++p) {
+                const LinePiece& pc = pieces[p];
+                for (int img = split; img < a.nimg; img += S) {
+                    double sx, sy, sz;
+                    if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
+                    line_piece_plane(pc, a.raw, px - sx, py - sy, pz - sz, acc.x, acc.y, acc.z);
+                }
             }
         }
     }
@@ -371,14 +443,43 @@ __global__ void __launch_bounds__(kThreads, Policy::kMinBlocks) field_kernel(con
 // One FP64 line piece: segments k0..k1e-1 of loop lp (segment k runs from
 // vertex k-1 to vertex k; Code/barnett.hpp:62-65), with everything that does
 // not depend on the atom precomputed; w is stored times cK = 1/(8 pi (1 - nu)).
-// rec is left to the chunk packer.
+// rec is left to the chunk packer.  The piece's input vertices (A of its
+// first segment, then every B) are appended to raw as x, y, z triplets; the
+// loop's mean plane (unit area vector n) and the largest distance of a vertex
+// from it give the band |n.(apex - P)| <= hband in which the kernel takes the
+// solid angle per triangle (a zero-area loop: everywhere).
 inline void make_line_piece(const disco_loop& lp, int k0, int k1e, double bx, double by, double bz,
-                            double cK, LinePiece& p, std::vector<LineSeg>& recs)
+                            double cK, LinePiece& p, std::vector<LineSeg>& recs, std::vector<double>& raw)
 {
     const int nv = lp.n_vertices;
     std::memset(&p, 0, sizeof(p));
     const int a = (k0 + nv - 1) % nv;
     const double c[3] = { lp.cx, lp.cy, lp.cz };
+    {
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int k = 0; k < nv; ++k) {
+            const int km = (k + nv - 1) % nv;
+            const double ux = lp.vx[km] - c[0], uy = lp.vy[km] - c[1], uz = lp.vz[km] - c[2];
+            const double vx = lp.vx[k] - c[0], vy = lp.vy[k] - c[1], vz = lp.vz[k] - c[2];
+            sx += uy * vz - uz * vy;
+            sy += uz * vx - ux * vz;
+            sz += ux * vy - uy * vx;
+        }
+        const double s = std::sqrt(sx * sx + sy * sy + sz * sz);
+        if (s > 0.0 && std::isfinite(s)) {
+            p.nx = sx / s; p.ny = sy / s; p.nz = sz / s;
+            double dev = 0.0;
+            for (int k = 0; k < nv; ++k)
+                dev = std::max(dev, std::fabs(p.nx * (lp.vx[k] - c[0]) + p.ny * (lp.vy[k] - c[1]) +
+                                              p.nz * (lp.vz[k] - c[2])));
+            p.hband = 2.0 * dev + 1e-8;
+        } else {
+            p.hband = HUGE_VAL;
+        }
+    }
+    p.raw = (int32_t)(raw.size() / 3);
+    raw.push_back(lp.vx[a]); raw.push_back(lp.vy[a]); raw.push_back(lp.vz[a]);
+    for (int k = k0; k < k1e; ++k) { raw.push_back(lp.vx[k]); raw.push_back(lp.vy[k]); raw.push_back(lp.vz[k]); }
     p.ax = lp.vx[a] - c[0]; p.ay = lp.vy[a] - c[1]; p.az = lp.vz[a] - c[2];
     p.cx = c[0]; p.cy = c[1]; p.cz = c[2];
     p.bx = bx; p.by = by; p.bz = bz;

@@ -54,6 +54,7 @@ int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, H
         PieceList<LinePieceF, LineSegF> L;
         std::vector<LinePiece> p64;
         std::vector<LineSeg> s64;
+        std::vector<double> raw;
         for (int l = 0; l < nloops; ++l) {
             const disco_loop& lp = loops[l];
             if (!lp.line) continue;
@@ -75,7 +76,7 @@ int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, H
                 const int a = (k0 + nv - 1) % nv;
                 LinePiece q;
                 std::vector<LineSeg> segs;
-                make_line_piece(lp, k0, k1e, bx, by, bz, k1, q, segs);
+                make_line_piece(lp, k0, k1e, bx, by, bz, k1, q, segs, raw);
                 q.rec = (int32_t)s64.size();
                 LinePieceF p;
                 std::memset(&p, 0, sizeof(p));
@@ -109,6 +110,7 @@ int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, H
             T.aux_pieces = T.bytes.size() - p64.size() * sizeof(LinePiece);
             append_aligned(T.bytes, s64.data(), s64.size() * sizeof(LineSeg));
             T.aux_segs = T.bytes.size() - s64.size() * sizeof(LineSeg);
+            append_raw(T, raw);
         }
     } else {
         PieceList<LooponPieceF, LooponRecF> L;

@@ -210,6 +210,7 @@ struct LineNearFp64 {
     {
         const LinePieceF* pieces = reinterpret_cast<const LinePieceF*>(st);
         const double cJK = a.cJ / a.cK;
+        bool plane = false;
         for (int p = 0; p < npieces; ++p) {
             const LinePieceF& pc = pieces[p];
             const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
@@ -220,7 +221,21 @@ struct LineNearFp64 {
                 if (!near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) continue;
                 const LinePiece& p64 = a.pieces64[pc.piece64];
                 line_piece_fp64(p64, a.segs64 + p64.rec, px - sx, py - sy, pz - sz, cJK,
-                                acc.x, acc.y, acc.z);
+                                acc.x, acc.y, acc.z, plane);
+            }
+        }
+        if (plane) {                        // an atom in a loop's plane band: the reference's solid angle
+            for (int p = 0; p < npieces; ++p) {
+                const LinePieceF& pc = pieces[p];
+                const double qx = px - pc.cx, qy = py - pc.cy, qz = pz - pc.cz;
+                for (int img = split; img < a.nimg; img += S) {
+                    double sx, sy, sz;
+                    if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
+                    const float Px = (float)(qx - sx), Py = (float)(qy - sy), Pz = (float)(qz - sz);
+                    if (!near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) continue;
+                    line_piece_plane(a.pieces64[pc.piece64], a.raw, px - sx, py - sy, pz - sz,
+                                     acc.x, acc.y, acc.z);
+                }
             }
         }
     }

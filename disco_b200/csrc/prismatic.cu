@@ -19,32 +19,27 @@
 //            written at base + tile offset + rank, i.e. ascending atom order.
 // A fourth single-CTA pass gathers the interstitial copies in loop order then
 // slab order, drops those of removed atoms and renumbers their sources.
+#include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
 
 namespace disco {
 
-constexpr int kSlabThreads = 256;
-constexpr int kSlabRounds = 8;
-constexpr int kSlabTile = kSlabThreads * kSlabRounds;   // atoms per tile
 constexpr int kMaxSlabLoops = 64;                       // active slab loops per call
-constexpr int kSlabWarps = kSlabThreads / 32;
 
 struct SlabLoopDev {
     disco_slab_loop L;
     double tLo, tHi;       // slab bounds in units of d (Code/prismatic.cpp:58-59)
     double cuv, det;       // u.v and 1 - (u.v)^2 (Code/loop.cpp:327-328)
-    float nf[3], cf[3];    // the pre-test only: n, c, 1 / spacing, its margin in planes
-    float inv_df, margin;
-    int32_t type;          // DISCO_MATTER_VACANCY or DISCO_MATTER_INTERSTITIAL
-    int32_t pad;
 };
 
 // ---- the predicate, FP64 round-to-nearest, reference operation order -------------------
@@ -94,35 +89,8 @@ __device__ bool inside_uv_rn(const disco_slab_loop& g, double u, double v)
     return __dadd_rn(__dmul_rn(du, du), __dmul_rn(dv, dv)) <= __dadd_rn(__dmul_rn(g.r_corner, g.r_corner), eps);
 }
 
-// Cheap pre-test in FP32: true only if the atom's t is outside [tLo, tHi) by
-// more than `margin` planes.  With the atom and the centre rounded to FP32
-// and the nearest image unambiguous (r/L + 1/2 at least 1e-5 from an integer
-// and |r/L| < 2, else it returns false), the FP32 t differs from the exactly
-// rounded t of slab_member by less than 1.5e-6 (Lx + Ly + Lz) / d + 1e-6
-// planes; the margin is 1e-5 (Lx + Ly + Lz) / d + 1e-3.  So it never rejects
-// a member: the exact test below decides every atom it passes, and atom sets
-// stay bit-exact.
-__device__ __forceinline__ bool clearly_outside(const SlabLoopDev& S, const float (&p)[3], const float (&L)[3],
-                                                const float (&iL)[3])
-{
-    float s = 0.0f;
-    bool sure = true;                     // branch-free, so that loops interleave
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float r = p[k] - S.cf[k];
-        const float q = r * iL[k];
-        const float h = q + 0.5f;
-        const float f = floorf(h);
-        const float fr = h - f;
-        sure = sure && fabsf(q) < 2.0f && fr >= 1e-5f && fr <= 1.0f - 1e-5f;
-        s = fmaf(S.nf[k], fmaf(-L[k], f, r), s);
-    }
-    const float t = s * S.inv_df;
-    return sure && (t < (float)S.tLo - S.margin || t >= (float)S.tHi + S.margin);
-}
-
 // Slab membership of one atom (Code/prismatic.cpp:61-72); side = sign of s.
-__device__ __forceinline__ bool slab_member(const SlabLoopDev& S, double x, double y, double z,
+__device__ __noinline__ bool slab_member(const SlabLoopDev& S, double x, double y, double z,
                                             double Lx, double Ly, double Lz, bool& pos_side)
 {
     const disco_slab_loop& g = S.L;
@@ -141,274 +109,412 @@ __device__ __forceinline__ bool slab_member(const SlabLoopDev& S, double x, doub
     return true;
 }
 
-struct SlabArgs {
+// Per-loop header staged in shared memory: what the tile culling and the FP32
+// pre-test read for every atom (the full record stays in global memory and is
+// read only for the exact test).
+struct SlabHead {
+    double cx, cy, cz;     // centre (FP64)
+    double bound;          // |r| of every slab member is below this (A)
+    float nf[3], cf[3];    // pre-test: n, c
+    float inv_df, margin;  // 1 / spacing, margin in planes
+    float tlo, thi;        // slab bounds in planes
+    int32_t type;          // DISCO_MATTER_VACANCY or DISCO_MATTER_INTERSTITIAL
+    int32_t pad;
+};
+static_assert(sizeof(SlabHead) == 80, "slab header layout");
+
+// One slab-member atom, in atom order: which loops' slabs it is in and on
+// which side, and whether a vacancy slab removes it.
+struct MemberRec {
+    int32_t atom;
+    int32_t removed;
+    uint64_t mask, sides;
+};
+
+constexpr int kMatterThreads = 512;
+constexpr int kMatterAtoms = 8;                                // per thread
+constexpr int kMatterTile = kMatterThreads * kMatterAtoms;     // 4096 atoms per tile
+constexpr int kMatterWarps = kMatterThreads / 32;
+constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // look-back categories
+
+// Look-back words: flag in the top two bits, value below.
+constexpr unsigned long long kFlagAgg = 1ull << 62;
+constexpr unsigned long long kFlagInc = 2ull << 62;
+constexpr unsigned long long kValMask = (1ull << 62) - 1;
+
+struct MatterArgs {
     const double *x, *y, *z;
     int64_t n;
-    const SlabLoopDev* loops;
-    int32_t nl;
+    const SlabHead* heads;        // [nl]
+    const SlabLoopDev* loops;     // [nl]
+    int32_t nl, C;                // C = 2 + 2 nl categories: survivors, members, slab of
+                                  // loop l (2 + l), kept copies of loop l (2 + nl + l)
     double Lx, Ly, Lz;
-    float iLx, iLy, iLz;      // 1 / box lengths in FP32 (the pre-test only)
-    int32_t* tile_counts;     // [ntiles][nl + 1]
-    int32_t* tile_offsets;    // [ntiles][nl + 1]
-    int64_t* totals;          // [nl + 1] totals, [nl] loop bases, [1] copies
+    float iLx, iLy, iLz;          // 1 / box lengths in FP32 (the pre-test only)
+    int32_t pad_;
+    unsigned long long* status;   // [ntiles][C] look-back words, zeroed per call
+    unsigned int* ticket;         // tile counter, zeroed per call
+    int32_t* tile_excl;           // [ntiles][C] exclusive prefixes
+    MemberRec* members;
+    int64_t member_cap;
     double *xo, *yo, *zo;
     int32_t* new_index;
     int32_t* slab_atoms;
     int8_t* slab_side;
+    int64_t slab_cap;
+    disco_copy* copies;
+    int64_t copy_cap;
+    int64_t* totals;              // [C] category totals (written by the tail)
+    int* err;
 };
 
-// Every atom's membership mask over the active loops, sides and removal.
-__device__ __forceinline__ void atom_masks(const SlabLoopDev* sl, int nl, double x, double y, double z,
-                                           const SlabArgs& a, uint64_t& mask, uint64_t& sides, bool& removed)
+__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v)
 {
-    const double Lx = a.Lx, Ly = a.Ly, Lz = a.Lz;
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Cheap pre-test in FP32: true only if the atom's t is outside [tLo, tHi) by
+// more than `margin` planes.  With the atom and the centre within 2 L of the
+// origin and rounded to FP32, and the nearest image unambiguous (r/L + 1/2 at
+// least 1e-5 from an integer and |r/L| < 2; else it returns false), the FP32
+// t differs from the exactly rounded t of slab_member by less than
+// 1.5e-6 (Lx + Ly + Lz) / d + 1e-6 planes; the margin is
+// 1e-5 (Lx + Ly + Lz) / d + 1e-3.  So it never rejects a member: the exact
+// test decides every atom it passes, and atom sets stay bit-exact.
+__device__ __forceinline__ bool clearly_outside(const SlabHead& S, const float (&p)[3], const float (&L)[3],
+                                                const float (&iL)[3])
+{
+    float s = 0.0f;
+    bool sure = true;                     // branch-free, so that loops interleave
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float r = p[k] - S.cf[k];
+        const float q = r * iL[k];
+        const float h = q + 0.5f;
+        const float f = floorf(h);
+        const float fr = h - f;
+        sure = sure && fabsf(q) < 2.0f && fr >= 1e-5f && fr <= 1.0f - 1e-5f &&
+               fabsf(p[k]) < 2.0f * L[k] && fabsf(S.cf[k]) < 2.0f * L[k];
+        s = fmaf(S.nf[k], fmaf(-L[k], f, r), s);
+    }
+    const float t = s * S.inv_df;
+    return sure && (t < S.tlo - S.margin || t >= S.thi + S.margin);
+}
+
+// Smallest |p - c - m L| over p in [lo, hi] and integers m, less a rounding
+// allowance (never above the true value).
+__device__ __forceinline__ double periodic_gap(double lo, double hi, double c, double L)
+{
+    const double a = lo - c, b = hi - c;
+    if (!(b - a < L)) return 0.0;
+    const double m1 = floor(a / L);
+    if ((m1 + 1.0) * L <= b) return 0.0;
+    const double d = fmin(a - m1 * L, (m1 + 1.0) * L - b);
+    return fmax(0.0, d - 1e-9 * L - 1e-6);
+}
+
+// Membership of one atom over the loops in `cand` (bits of loops whose slab
+// the tile can reach): the FP32 pre-test, then the exact FP64 test in loop order.
+__device__ __forceinline__ void atom_masks(const SlabHead* sh, const SlabLoopDev* sl, uint64_t cand, double x,
+                                           double y, double z, const MatterArgs& a, uint64_t& mask,
+                                           uint64_t& sides, bool& removed)
+{
     mask = 0; sides = 0; removed = false;
-    const float L[3] = { (float)Lx, (float)Ly, (float)Lz };
+    if (!cand) return;
+    const float L[3] = { (float)a.Lx, (float)a.Ly, (float)a.Lz };
     const float iL[3] = { a.iLx, a.iLy, a.iLz };
     const float p[3] = { (float)x, (float)y, (float)z };
-    // the pre-test for every loop first (independent, interleaved), then the
-    // exact test for the loops it could not exclude, in loop order
-    uint64_t cand = 0;
-#pragma unroll 4
-    for (int l = 0; l < nl; ++l)
-        if (!clearly_outside(sl[l], p, L, iL)) cand |= 1ull << l;
-    while (cand) {
-        const int l = __ffsll((long long)cand) - 1;
-        cand &= cand - 1;
+    uint64_t c2 = 0;
+    for (uint64_t c = cand; c; c &= c - 1) {
+        const int l = __ffsll((long long)c) - 1;
+        if (!clearly_outside(sh[l], p, L, iL)) c2 |= 1ull << l;
+    }
+    while (c2) {
+        const int l = __ffsll((long long)c2) - 1;
+        c2 &= c2 - 1;
         bool ps = false;
-        if (slab_member(sl[l], x, y, z, Lx, Ly, Lz, ps)) {
+        if (slab_member(sl[l], x, y, z, a.Lx, a.Ly, a.Lz, ps)) {
             mask |= 1ull << l;
             if (ps) sides |= 1ull << l;
-            if (sl[l].type == DISCO_MATTER_VACANCY) removed = true;
+            if (sh[l].type == DISCO_MATTER_VACANCY) removed = true;
         }
     }
 }
 
-__device__ __forceinline__ void load_loops(SlabLoopDev* dst, const SlabLoopDev* src, int nl)
+// The matter step's single pass over the atoms.  Each CTA takes the next tile
+// of 4096 atoms (a ticket, so that every tile it looks back on belongs to a
+// CTA already running), reads its atoms once, computes every atom's slab mask
+// once (loops whose slab cannot reach the tile's bounding box are skipped for
+// the whole tile), counts per category, obtains its exclusive prefixes by
+// decoupled look-back over the preceding tiles' published counts, and writes
+// the survivors (x, y, z, new index) and the slab members' records at their
+// final ranks.  Bounded waits: a look-back that finds no count for 2 s
+// records DISCO_ETIMEOUT and publishes anyway, so no tile waits forever.
+__global__ void __launch_bounds__(kMatterThreads, 1) matter_pass_kernel(const MatterArgs a)
 {
-    const int words = nl * (int)(sizeof(SlabLoopDev) / 8);
-    const uint64_t* s = reinterpret_cast<const uint64_t*>(src);
-    uint64_t* d = reinterpret_cast<uint64_t*>(dst);
-    for (int i = threadIdx.x; i < words; i += blockDim.x) d[i] = s[i];
-}
-
-// CTA b takes tiles b, b + grid, ... (with the grid of slab_grid: tile b).
-__global__ void __launch_bounds__(kSlabThreads) slab_count_kernel(const SlabArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SlabLoopDev* sl = reinterpret_cast<SlabLoopDev*>(smem_raw);
-    __shared__ int cnt[kMaxSlabLoops + 1];
-    const int C = a.nl + 1;
-    load_loops(sl, a.loops, a.nl);
-    const int lane = threadIdx.x & 31;
-    const int64_t ntiles = (a.n + kSlabTile - 1) / kSlabTile;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        for (int i = threadIdx.x; i < C; i += blockDim.x) cnt[i] = 0;
-        __syncthreads();
-        const int64_t base = tile * kSlabTile;
-        for (int r = 0; r < kSlabRounds; ++r) {
-            const int64_t i = base + r * kSlabThreads + threadIdx.x;
-            const bool valid = i < a.n;
-            uint64_t mask = 0, sides = 0;
-            bool removed = false;
-            if (valid) atom_masks(sl, a.nl, a.x[i], a.y[i], a.z[i], a, mask, sides, removed);
-            const unsigned b0 = __ballot_sync(0xffffffffu, valid && !removed);
-            if (lane == 0 && b0) atomicAdd(&cnt[0], __popc(b0));
-            for (int l = 0; l < a.nl; ++l) {
-                const unsigned b = __ballot_sync(0xffffffffu, (mask >> l) & 1ull);
-                if (lane == 0 && b) atomicAdd(&cnt[1 + l], __popc(b));
-            }
-        }
-        __syncthreads();
-        for (int c = threadIdx.x; c < C; c += blockDim.x)
-            a.tile_counts[tile * C + c] = cnt[c];
-        __syncthreads();
+    __shared__ SlabHead sh[kMaxSlabLoops];
+    __shared__ double red[6][kMatterWarps];
+    __shared__ unsigned long long tmask_s;
+    __shared__ int cnt_s[kMatterAtoms * kMatterWarps];         // survivors per (round, warp), then prefixes
+    __shared__ int cnt_m[kMatterAtoms * kMatterWarps];         // members per (round, warp), then prefixes
+    __shared__ int cnt_c[2 * kMaxSlabLoops];                   // slab and kept-copy counts per loop
+    __shared__ int64_t excl[kMaxCats];
+    __shared__ int tile_s;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nl = a.nl, C = a.C;
+    if (tid == 0) { tile_s = (int)atomicAdd(a.ticket, 1u); tmask_s = 0ull; }
+    {
+        const int words = nl * (int)(sizeof(SlabHead) / 8);
+        const uint64_t* src = reinterpret_cast<const uint64_t*>(a.heads);
+        uint64_t* dst = reinterpret_cast<uint64_t*>(sh);
+        for (int i = tid; i < words; i += kMatterThreads) dst[i] = src[i];
+        for (int i = tid; i < 2 * nl; i += kMatterThreads) cnt_c[i] = 0;
     }
-}
-
-// One CTA per category (survivors, then each loop): exclusive scan over the
-// tiles, the category's total; the last CTA to finish (a counter in
-// totals[2 C], zeroed with the totals) writes the loops' bases.
-__global__ void __launch_bounds__(1024) slab_scan_kernel(const SlabArgs a, int64_t ntiles)
-{
-    __shared__ int64_t warp_sum[32];
-    __shared__ int64_t carry;
-    __shared__ bool last;
-    const int C = a.nl + 1;
-    const int c = blockIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (int64_t t0 = 0; t0 < ntiles; t0 += blockDim.x) {
-        const int64_t t = t0 + threadIdx.x;
-        const int64_t v = t < ntiles ? a.tile_counts[t * C + c] : 0;
-        int64_t x = v;
+    const int64_t tile = tile_s;
+    const int64_t base = tile * kMatterTile;
+
+    // the tile's bounding box (the atoms are read from HBM here; the two later
+    // passes over the same 96 KB find them in L1/L2)
+    double lo[3] = { 1e300, 1e300, 1e300 }, hi[3] = { -1e300, -1e300, -1e300 };
+#pragma unroll
+    for (int r = 0; r < kMatterAtoms; ++r) {
+        const int64_t i = base + r * kMatterThreads + tid;
+        if (i < a.n) {
+            const double px = a.x[i], py = a.y[i], pz = a.z[i];
+            lo[0] = fmin(lo[0], px); hi[0] = fmax(hi[0], px);
+            lo[1] = fmin(lo[1], py); hi[1] = fmax(hi[1], py);
+            lo[2] = fmin(lo[2], pz); hi[2] = fmax(hi[2], pz);
+        }
+    }
+    if (nl > 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            for (int o = 16; o > 0; o >>= 1) {
+                lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+                hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+            }
+        if (lane == 0)
+            for (int k = 0; k < 3; ++k) { red[k][warp] = lo[k]; red[3 + k][warp] = hi[k]; }
+        __syncthreads();
+        if (tid < nl) {
+            double b[6];
+            for (int k = 0; k < 3; ++k) {
+                b[k] = red[k][0]; b[3 + k] = red[3 + k][0];
+                for (int w = 1; w < kMatterWarps; ++w) {
+                    b[k] = fmin(b[k], red[k][w]);
+                    b[3 + k] = fmax(b[3 + k], red[3 + k][w]);
+                }
+            }
+            const SlabHead& S = sh[tid];
+            const double gx = periodic_gap(b[0], b[3], S.cx, a.Lx);
+            const double gy = periodic_gap(b[1], b[4], S.cy, a.Ly);
+            const double gz = periodic_gap(b[2], b[5], S.cz, a.Lz);
+            if (!(gx * gx + gy * gy + gz * gz > S.bound * S.bound)) atomicOr(&tmask_s, 1ull << tid);
+        }
+        __syncthreads();
+    }
+    const uint64_t tmask = tmask_s;
+
+    // every atom's mask, once
+    uint64_t mask[kMatterAtoms], sides[kMatterAtoms];
+    unsigned rem = 0, val = 0;
+#pragma unroll
+    for (int r = 0; r < kMatterAtoms; ++r) {
+        const int64_t i = base + r * kMatterThreads + tid;
+        bool removed = false;
+        mask[r] = 0; sides[r] = 0;
+        if (i < a.n) {
+            val |= 1u << r;
+            if (tmask) atom_masks(sh, a.loops, tmask, a.x[i], a.y[i], a.z[i], a, mask[r], sides[r], removed);
+        }
+        if (removed) rem |= 1u << r;
+        const unsigned bs = __ballot_sync(0xffffffffu, ((val >> r) & 1u) && !removed);
+        const unsigned bm = __ballot_sync(0xffffffffu, mask[r] != 0);
+        if (lane == 0) { cnt_s[r * kMatterWarps + warp] = __popc(bs); cnt_m[r * kMatterWarps + warp] = __popc(bm); }
+        for (uint64_t m = mask[r]; m; m &= m - 1) {            // members are rare
+            const int l = __ffsll((long long)m) - 1;
+            atomicAdd(&cnt_c[l], 1);
+            if (sh[l].type == DISCO_MATTER_INTERSTITIAL && !removed) atomicAdd(&cnt_c[nl + l], 1);
+        }
+    }
+    __syncthreads();
+
+    // tile totals, then prefixes over (round, warp) in atom order
+    if (warp == 0 || warp == 1) {
+        int* cnt = warp == 0 ? cnt_s : cnt_m;
+        constexpr int kPer = kMatterAtoms * kMatterWarps / 32;  // 4 entries per lane
+        int v[kPer], tot = 0;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) { v[j] = cnt[lane * kPer + j]; tot += v[j]; }
+        int incl = tot;
         for (int o = 1; o < 32; o <<= 1) {
-            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
         }
-        if (lane == 31) warp_sum[warp] = x;
-        __syncthreads();
-        if (warp == 0) {
-            int64_t s = lane < (int)(blockDim.x >> 5) ? warp_sum[lane] : 0;
-            for (int o = 1; o < 32; o <<= 1) {
-                const int64_t y = __shfl_up_sync(0xffffffffu, s, o);
-                if (lane >= o) s += y;
-            }
-            warp_sum[lane] = s;           // inclusive over warps
-        }
-        __syncthreads();
-        const int64_t excl = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + x - v;
-        if (t < ntiles) a.tile_offsets[t * C + c] = (int32_t)excl;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += warp_sum[(blockDim.x >> 5) - 1];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        a.totals[c] = carry;
-        __threadfence();
-        const unsigned long long done =
-            atomicAdd(reinterpret_cast<unsigned long long*>(&a.totals[2 * C]), 1ull);
-        last = done == (unsigned long long)(C - 1);
+        int run = incl - tot;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) { cnt[lane * kPer + j] = run; run += v[j]; }
+        if (lane == 31) excl[warp] = incl;                     // tile aggregate (temporarily)
     }
     __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        const volatile int64_t* tot = a.totals;
-        int64_t acc = 0;
-        for (int l = 0; l < a.nl; ++l) { a.totals[C + l] = acc; acc += tot[1 + l]; }
-    }
-}
 
-__global__ void __launch_bounds__(kSlabThreads) slab_scatter_kernel(const SlabArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SlabLoopDev* sl = reinterpret_cast<SlabLoopDev*>(smem_raw);
-    __shared__ int wcnt[kSlabWarps][kMaxSlabLoops + 1];    // per-warp counts, then prefixes
-    __shared__ int run[kMaxSlabLoops + 1];                 // running count within the tile
-    __shared__ int64_t base_off[kMaxSlabLoops + 1];        // global offset of this tile per category
-    const int C = a.nl + 1;
-    load_loops(sl, a.loops, a.nl);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned lt = (1u << lane) - 1u;
-    const int64_t ntiles = (a.n + kSlabTile - 1) / kSlabTile;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        for (int c = threadIdx.x; c < C; c += blockDim.x) {
-            run[c] = 0;
-            const int64_t t = a.tile_offsets[tile * C + c];
-            base_off[c] = c == 0 ? t : a.totals[C + (c - 1)] + t;
+    // decoupled look-back, one thread per category
+    if (tid < C) {
+        const int c = tid;
+        const int64_t agg = c == 0 ? excl[0] : c == 1 ? excl[1] : (int64_t)cnt_c[c - 2];
+        unsigned long long* my = a.status + tile * C + c;
+        int64_t prefix = 0;
+        if (tile == 0) {
+            st_release(my, kFlagInc | (unsigned long long)agg);
+        } else {
+            st_release(my, kFlagAgg | (unsigned long long)agg);
+            int64_t j = tile - 1;
+            unsigned long long t0 = 0;
+            while (true) {
+                const unsigned long long v = ld_acquire(a.status + j * C + c);
+                const unsigned long long f = v & ~kValMask;
+                if (f == 0) {
+                    if (t0 == 0) t0 = global_ns();
+                    else if (global_ns() - t0 > kWaitLimitNs) { report(a.err, DISCO_ETIMEOUT); break; }
+                    continue;
+                }
+                prefix += (int64_t)(v & kValMask);
+                if (f == kFlagInc || j == 0) break;
+                --j;
+                t0 = 0;
+            }
+            st_release(my, kFlagInc | (unsigned long long)(prefix + agg));
         }
-        __syncthreads();
-        const int64_t base = tile * kSlabTile;
-        for (int r = 0; r < kSlabRounds; ++r) {
-            const int64_t i = base + r * kSlabThreads + threadIdx.x;
-            const bool valid = i < a.n;
-            uint64_t mask = 0, sides = 0;
-            bool removed = false;
-            double x = 0., y = 0., z = 0.;
-            if (valid) {
-                x = a.x[i]; y = a.y[i]; z = a.z[i];
-                atom_masks(sl, a.nl, x, y, z, a, mask, sides, removed);
+        a.tile_excl[tile * C + c] = (int32_t)prefix;
+        excl[c] = prefix;
+    }
+    __syncthreads();
+
+    // survivors at their final ranks, the new-index map, member records
+    const unsigned ltm = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kMatterAtoms; ++r) {
+        const int64_t i = base + r * kMatterThreads + tid;
+        const bool valid = (val >> r) & 1u;
+        const bool surv = valid && !((rem >> r) & 1u);
+        const unsigned bs = __ballot_sync(0xffffffffu, surv);
+        const unsigned bm = __ballot_sync(0xffffffffu, mask[r] != 0);
+        if (valid) {
+            if (surv) {
+                const int64_t q = excl[0] + cnt_s[r * kMatterWarps + warp] + __popc(bs & ltm);
+                if (q < a.n) { a.xo[q] = a.x[i]; a.yo[q] = a.y[i]; a.zo[q] = a.z[i]; }
+                a.new_index[i] = (int32_t)q;
+            } else {
+                a.new_index[i] = -1;
             }
-            const bool surv = valid && !removed;
-            const unsigned b0 = __ballot_sync(0xffffffffu, surv);
-            const int r0 = __popc(b0 & lt);
-            if (lane == 0) wcnt[warp][0] = __popc(b0);
-            for (int l = 0; l < a.nl; ++l) {
-                const unsigned b = __ballot_sync(0xffffffffu, (mask >> l) & 1ull);
-                if (lane == 0) wcnt[warp][1 + l] = __popc(b);
+        }
+        if (mask[r]) {
+            const int64_t q = excl[1] + cnt_m[r * kMatterWarps + warp] + __popc(bm & ltm);
+            if (q < a.member_cap) {
+                MemberRec m;
+                m.atom = (int32_t)i;
+                m.removed = (rem >> r) & 1u;
+                m.mask = mask[r];
+                m.sides = sides[r];
+                a.members[q] = m;
             }
-            __syncthreads();
-            // exclusive prefix over the warps of this round, per category
-            for (int c = threadIdx.x; c < C; c += blockDim.x) {
-                int acc = run[c];
-                for (int w = 0; w < kSlabWarps; ++w) {
-                    const int v = wcnt[w][c];
-                    wcnt[w][c] = acc;
-                    acc += v;
-                }
-                run[c] = acc;
-            }
-            __syncthreads();
-            if (valid) {
-                if (surv) {
-                    const int64_t p = base_off[0] + wcnt[warp][0] + r0;
-                    a.xo[p] = x; a.yo[p] = y; a.zo[p] = z;
-                    a.new_index[i] = (int32_t)p;
-                } else {
-                    a.new_index[i] = -1;
-                }
-            }
-            for (int l = 0; l < a.nl; ++l) {
-                const bool m = (mask >> l) & 1ull;
-                const unsigned b = __ballot_sync(0xffffffffu, m);
-                if (m) {
-                    const int64_t p = base_off[1 + l] + wcnt[warp][1 + l] + __popc(b & lt);
-                    a.slab_atoms[p] = (int32_t)i;
-                    a.slab_side[p] = ((sides >> l) & 1ull) ? 1 : -1;
-                }
-            }
-            __syncthreads();
         }
     }
 }
 
-// One CTA: interstitial copies in loop order then slab order (Code/main.cpp:
-// 651-654), copies of removed atoms dropped and sources renumbered (:676-679).
-__global__ void __launch_bounds__(1024) slab_copies_kernel(const SlabArgs a, disco_copy* copies,
-                                                           int64_t copy_capacity)
+// The slab entries and the interstitial copies, from the member records of
+// one tile (CTA t <-> tile t, after the pass has finished): entry of loop l
+// at loop base + the tile's exclusive count of loop l + its rank among the
+// tile's members in l (ascending atom order, Code/prismatic.cpp:61-72); a copy
+// of an interstitial loop's entry whose atom survives at copy base + the tile's
+// exclusive kept count + its rank (loop order, then slab order; sources
+// renumbered, Code/main.cpp:651-654,676-679).  CTA 0 also writes the totals.
+__global__ void __launch_bounds__(256) matter_tail_kernel(const MatterArgs a, int64_t ntiles)
 {
-    __shared__ int warp_sum[32];
-    __shared__ int64_t carry;
-    const int C = a.nl + 1;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) carry = 0;
+    __shared__ int64_t tot[kMaxCats];
+    __shared__ int64_t lbase[kMaxSlabLoops], cbase[kMaxSlabLoops];
+    __shared__ int run[2 * kMaxSlabLoops];
+    __shared__ int wc[8][2];
+    __shared__ unsigned long long umask;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nl = a.nl, C = a.C;
+    const int64_t t = blockIdx.x;
+    const int64_t m0 = a.tile_excl[t * C + 1];                       // this tile's member records
+    const int64_t mend = (int64_t)(a.status[t * C + 1] & kValMask);  // its inclusive count
+    if (t != 0 && mend == m0) return;
+    // totals = the last tile's inclusive counts; loop and copy bases
+    for (int c = tid; c < C; c += 256) tot[c] = (int64_t)(a.status[(ntiles - 1) * C + c] & kValMask);
+    if (tid == 0) umask = 0ull;
+    for (int i = tid; i < 2 * nl; i += 256) run[i] = 0;
     __syncthreads();
-    for (int l = 0; l < a.nl; ++l) {
-        if (a.loops[l].type != DISCO_MATTER_INTERSTITIAL) continue;
-        const int64_t b0 = a.totals[C + l], cnt = a.totals[1 + l];
-        const disco_slab_loop& g = a.loops[l].L;
-        for (int64_t e0 = 0; e0 < cnt; e0 += blockDim.x) {
-            const int64_t e = e0 + threadIdx.x;
-            int32_t src = -1;
-            int8_t side = 1;
-            if (e < cnt) {
-                const int32_t atom = a.slab_atoms[b0 + e];
-                side = a.slab_side[b0 + e];
-                src = a.new_index[atom];
-            }
-            const bool keep = src >= 0;
-            const unsigned bal = __ballot_sync(0xffffffffu, keep);
-            if (lane == 0) warp_sum[warp] = __popc(bal);
+    if (tid == 0) {
+        int64_t sb = 0, cb = 0;
+        for (int l = 0; l < nl; ++l) {
+            lbase[l] = sb; sb += tot[2 + l];
+            cbase[l] = cb; cb += tot[2 + nl + l];
+        }
+        if (t == 0) {
+            for (int c = 0; c < C; ++c) a.totals[c] = tot[c];
+            a.totals[C] = *a.err;                              // the pass's error word
+        }
+    }
+    __syncthreads();
+    for (int64_t e0 = m0; e0 < mend; e0 += 256) {
+        const int64_t e = e0 + tid;
+        MemberRec m;
+        m.atom = 0; m.removed = 1; m.mask = 0; m.sides = 0;
+        if (e < mend && e < a.member_cap) m = a.members[e];
+        if (m.mask) atomicOr(&umask, m.mask);
+        __syncthreads();
+        const uint64_t um = umask;
+        for (uint64_t u = um; u; u &= u - 1) {
+            const int l = __ffsll((long long)u) - 1;
+            const bool in = (m.mask >> l) & 1ull;
+            const bool keep = in && !m.removed && a.heads[l].type == DISCO_MATTER_INTERSTITIAL;
+            const unsigned bi = __ballot_sync(0xffffffffu, in);
+            const unsigned bk = __ballot_sync(0xffffffffu, keep);
+            if (lane == 0) { wc[warp][0] = __popc(bi); wc[warp][1] = __popc(bk); }
             __syncthreads();
-            if (warp == 0) {
-                int s = lane < (int)(blockDim.x >> 5) ? warp_sum[lane] : 0;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, s, o);
-                    if (lane >= o) s += y;
+            int pi = run[l], pk = run[nl + l];
+            for (int w = 0; w < warp; ++w) { pi += wc[w][0]; pk += wc[w][1]; }
+            const unsigned ltm = (1u << lane) - 1u;
+            if (in) {
+                const int64_t q = lbase[l] + a.tile_excl[t * C + 2 + l] + pi + __popc(bi & ltm);
+                if (q < a.slab_cap) {
+                    a.slab_atoms[q] = m.atom;
+                    a.slab_side[q] = ((m.sides >> l) & 1ull) ? 1 : -1;
                 }
-                warp_sum[lane] = s;
             }
-            __syncthreads();
             if (keep) {
-                const int64_t p = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + __popc(bal & ((1u << lane) - 1u));
-                if (p < copy_capacity) {
+                const int64_t q = cbase[l] + a.tile_excl[t * C + 2 + nl + l] + pk + __popc(bk & ltm);
+                if (q < a.copy_cap) {
+                    const disco_slab_loop& g = a.loops[l].L;
+                    const double* sh = ((m.sides >> l) & 1ull) ? g.shift_pos : g.shift_neg;
                     disco_copy cp;
-                    cp.atom = src;
+                    cp.atom = a.new_index[m.atom];
                     cp.reserved = 0;
-                    const double* sh = side > 0 ? g.shift_pos : g.shift_neg;
                     cp.shift[0] = sh[0]; cp.shift[1] = sh[1]; cp.shift[2] = sh[2];
-                    copies[p] = cp;
+                    a.copies[q] = cp;
                 }
             }
             __syncthreads();
-            if (threadIdx.x == 0) carry += warp_sum[(blockDim.x >> 5) - 1];
+            if (tid == 0) {
+                for (int w = 0; w < 8; ++w) { run[l] += wc[w][0]; run[nl + l] += wc[w][1]; }
+            }
             __syncthreads();
         }
+        if (tid == 0) umask = 0ull;
+        __syncthreads();
     }
-    if (threadIdx.x == 0) a.totals[2 * C - 1] = carry;   // slot after the loop bases
 }
-
 // Code/main.cpp:733-743 + 797-818: copies appended with u(src) + shift, then
 // r = x + u folded once into [-L/2, L/2] and shifted by +L/2.
 __global__ void finalize_kernel(const double* __restrict__ x, const double* __restrict__ y,
@@ -460,18 +566,10 @@ int efail(int code, const std::string& msg)
     return code;
 }
 
-// Grid of the tile kernels: one CTA per tile (a persistent grid of 4 CTAs
-// per SM measured 25 % slower: the per-round barriers of a tile want as many
-// CTAs in flight as the GPU holds).
-unsigned slab_grid(int64_t ntiles)
-{
-    return (unsigned)ntiles;
-}
-
 // One loop's SlabResult scalars (Code/prismatic.cpp:42-57) and, when it is
-// active (b.n != 0 and apply), its device record.  Never allocates.
-int slab_loop_record(const disco_slab_loop& g, int l, const double box[3], disco_slab_info& in,
-                     disco::SlabLoopDev& d, bool& active)
+// active (b.n != 0 and apply), its device header and record.  Never allocates.
+int slab_loop_record(const disco_slab_loop& g, const double box[3], disco_slab_info& in,
+                     disco::SlabHead& h, disco::SlabLoopDev& d, bool& active)
 {
     std::memset(&in, 0, sizeof(in));
     active = false;
@@ -483,7 +581,6 @@ int slab_loop_record(const disco_slab_loop& g, int l, const double box[3], disco
     if (!g.apply || type == DISCO_MATTER_NONE) return DISCO_OK;
     if (g.shape < 0 || g.shape > DISCO_SHAPE_POLYGON || g.n_poly < 0 || g.n_poly > DISCO_MAX_POLY ||
         !(g.spacing > 0.)) {
-        (void)l;
         disco::set_last_error("bad slab loop: shape, polygon size or spacing out of range");
         return DISCO_EINVAL;
     }
@@ -504,34 +601,172 @@ int slab_loop_record(const disco_slab_loop& g, int l, const double box[3], disco
     const double c = g.u[0] * g.v[0] + g.u[1] * g.v[1] + g.u[2] * g.v[2];
     d.cuv = c;
     d.det = 1.0 - c * c;
+
+    std::memset(&h, 0, sizeof(h));
+    h.cx = g.c[0]; h.cy = g.c[1]; h.cz = g.c[2];
     for (int k = 0; k < 3; ++k) {
-        d.nf[k] = (float)g.n[k];
-        d.cf[k] = (float)g.c[k];
+        h.nf[k] = (float)g.n[k];
+        h.cf[k] = (float)g.c[k];
     }
-    d.inv_df = (float)(1.0 / in.spacing);
-    d.margin = (float)(1e-5 * (box[0] + box[1] + box[2]) / in.spacing + 1e-3);
-    d.type = type;
+    h.inv_df = (float)(1.0 / in.spacing);
+    h.margin = (float)(1e-5 * (box[0] + box[1] + box[2]) / in.spacing + 1e-3);
+    h.tlo = (float)d.tLo;
+    h.thi = (float)d.tHi;
+    h.type = type;
+    // Bound on |r| (minimum image) of a member: the in-plane test holds for
+    // (uu, vv) within rho of the origin (Code/loop.cpp:281-316), r = uu u + vv v
+    // + s n with |s| <= max(|tLo|, tHi) d when u, v are unit vectors orthogonal
+    // to n, and |uu u + vv v| <= rho sqrt(1 + |u.v|).  Any other frame: no bound.
+    double rho;
+    if (g.shape == DISCO_SHAPE_CIRCLE) {
+        rho = g.radius;
+    } else if (g.shape == DISCO_SHAPE_POLYGON) {
+        rho = 0.0;
+        for (int i = 0; i < g.n_poly; ++i)
+            rho = std::max(rho, std::max(std::hypot(g.pu[i], g.pv[i]), std::hypot(g.qu[i], g.qv[i])));
+        rho += std::max(g.r_corner, 0.0);
+    } else {
+        rho = std::hypot(g.half_m, g.half_p) + std::max(g.r_corner, 0.0);
+    }
+    const double uu = g.u[0] * g.u[0] + g.u[1] * g.u[1] + g.u[2] * g.u[2];
+    const double vv = g.v[0] * g.v[0] + g.v[1] * g.v[1] + g.v[2] * g.v[2];
+    const double nn = g.n[0] * g.n[0] + g.n[1] * g.n[1] + g.n[2] * g.n[2];
+    const double un = g.u[0] * g.n[0] + g.u[1] * g.n[1] + g.u[2] * g.n[2];
+    const double vn = g.v[0] * g.n[0] + g.v[1] * g.n[1] + g.v[2] * g.n[2];
+    const bool frame = std::fabs(uu - 1.0) < 1e-9 && std::fabs(vv - 1.0) < 1e-9 && std::fabs(nn - 1.0) < 1e-9 &&
+                       std::fabs(un) < 1e-9 && std::fabs(vn) < 1e-9 && std::isfinite(rho);
+    const double smax = std::max(std::fabs(d.tLo), std::fabs(d.tHi)) * in.spacing;
+    h.bound = frame ? (rho * std::sqrt(1.0 + std::fabs(c)) + smax) * (1.0 + 1e-9) + 1e-6 +
+                      1e-9 * (box[0] + box[1] + box[2])
+                    : HUGE_VAL;
     active = true;
     return DISCO_OK;
 }
 
-// Active loops in caller order.
+// Active loops in caller order into heads[] / recs[] (capacity kMaxSlabLoops).
 int prepare_loops(const disco_slab_loop* loops, int nloops, const double box[3], disco_slab_info* info,
-                  std::vector<disco::SlabLoopDev>& act, std::vector<int>& act_index)
+                  disco::SlabHead* heads, disco::SlabLoopDev* recs, int* act_index, int& nl)
 {
+    nl = 0;
     for (int l = 0; l < nloops; ++l) {
-        disco::SlabLoopDev d;
         bool active = false;
-        const int st = slab_loop_record(loops[l], l, box, info[l], d, active);
+        disco::SlabHead h;
+        disco::SlabLoopDev d;
+        const int st = slab_loop_record(loops[l], box, info[l], h, d, active);
         if (st) return st;
         if (!active) continue;
-        if ((int)act.size() >= disco::kMaxSlabLoops) {
+        if (nl >= disco::kMaxSlabLoops) {
             disco::set_last_error("more than 64 prismatic loops in one call");
             return DISCO_ELIMIT;
         }
-        act.push_back(d);
-        act_index.push_back(l);
+        heads[nl] = h;
+        recs[nl] = d;
+        act_index[nl++] = l;
     }
+    return DISCO_OK;
+}
+
+// Host staging of the loop headers and records of one call: headers, then the
+// records at recs_offset(nl), filled and uploaded with a single copy while
+// g_stage_mutex is held (never from the stack).
+struct LoopStage {
+    disco::SlabHead heads[disco::kMaxSlabLoops];
+    disco::SlabLoopDev recs[disco::kMaxSlabLoops];
+};
+std::mutex g_stage_mutex;
+LoopStage g_stage_parts;
+unsigned char g_stage_bytes[sizeof(LoopStage)];
+
+size_t recs_offset(int nl) { return ((size_t)nl * sizeof(disco::SlabHead) + 15) & ~size_t(15); }
+
+// prepare_loops into the staging buffer, then one upload of its used bytes
+// to dst on stream s.
+int stage_loops(const disco_slab_loop* loops, int nloops, const double box[3], disco_slab_info* info,
+                int* act_index, int& nl, unsigned char* dst, cudaStream_t s)
+{
+    std::lock_guard<std::mutex> lock(g_stage_mutex);
+    int st = prepare_loops(loops, nloops, box, info, g_stage_parts.heads, g_stage_parts.recs, act_index, nl);
+    if (st || nl == 0) return st;
+    const size_t hb = (size_t)nl * sizeof(disco::SlabHead), off = recs_offset(nl);
+    std::memcpy(g_stage_bytes, g_stage_parts.heads, hb);
+    std::memset(g_stage_bytes + hb, 0, off - hb);
+    std::memcpy(g_stage_bytes + off, g_stage_parts.recs, (size_t)nl * sizeof(disco::SlabLoopDev));
+    const cudaError_t e = cudaMemcpyAsync(dst, g_stage_bytes, off + (size_t)nl * sizeof(disco::SlabLoopDev),
+                                          cudaMemcpyHostToDevice, s);
+    return e == cudaSuccess ? DISCO_OK : cfail(e, "loop table upload");
+}
+
+// Bytes of the look-back words (ticket and error word first).
+size_t status_bytes(int64_t ntiles, int C) { return 16 + (size_t)ntiles * C * sizeof(unsigned long long); }
+
+struct MatterScratch {
+    unsigned char* loops;        // heads then records (sizeof(LoopStage))
+    unsigned char* status;       // status_bytes(ntiles, C)
+    int32_t* tile_excl;          // ntiles * C
+    disco::MemberRec* members;
+    int64_t member_cap;
+    int64_t* totals;             // C + 1 (the last: the kernels' error word)
+};
+
+// Queues the matter step on stream s after stage_loops (no host wait): the
+// look-back words cleared, the single pass, the tail.
+int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int64_t ntiles, cudaStream_t s)
+{
+    using namespace disco;
+    cudaError_t e = cudaSuccess;
+    a.heads = reinterpret_cast<const SlabHead*>(m.loops);
+    a.loops = reinterpret_cast<const SlabLoopDev*>(m.loops + recs_offset(nl));
+    a.nl = nl;
+    a.C = 2 + 2 * nl;
+    a.status = reinterpret_cast<unsigned long long*>(m.status + 16);
+    a.ticket = reinterpret_cast<unsigned int*>(m.status);
+    a.err = reinterpret_cast<int*>(m.status + 4);
+    a.tile_excl = m.tile_excl;
+    a.members = m.members;
+    a.member_cap = m.member_cap;
+    a.totals = m.totals;
+    e = cudaMemsetAsync(m.status, 0, status_bytes(ntiles, a.C), s);
+    if (e != cudaSuccess) return cfail(e, "look-back reset");
+    if (ntiles > 0) {
+        matter_pass_kernel<<<(unsigned)ntiles, kMatterThreads, 0, s>>>(a);
+        matter_tail_kernel<<<(unsigned)ntiles, 256, 0, s>>>(a, ntiles);
+    } else {
+        e = cudaMemsetAsync(m.totals, 0, (size_t)(a.C + 1) * sizeof(int64_t), s);
+        if (e != cudaSuccess) return cfail(e, "totals reset");
+    }
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cfail(e, "matter step launch");
+    return DISCO_OK;
+}
+
+// After the stream has reached the end of the step: counts, info offsets and
+// the capacity checks from the totals (host copy tot[0..C], tot[C] = error).
+int matter_finish(const int64_t* tot, int nl, const int* act_index, int nloops, disco_slab_info* info,
+                  int64_t slab_capacity, int64_t copy_capacity, int64_t member_cap, int64_t counts[3])
+{
+    if (tot[2 + 2 * nl]) return efail(DISCO_ETIMEOUT, "matter step: a bounded device wait gave up");
+    int64_t slab_total = 0, copy_total = 0;
+    for (int q = 0; q < nl; ++q) {
+        disco_slab_info& in = info[act_index[q]];
+        in.offset = slab_total;
+        in.count = tot[2 + q];
+        slab_total += tot[2 + q];
+        copy_total += tot[2 + nl + q];
+    }
+    {
+        int64_t next = slab_total;       // inactive loops: empty range where the next active one starts
+        for (int l = nloops - 1; l >= 0; --l) {
+            if (info[l].type == DISCO_MATTER_NONE) info[l].offset = next;
+            else next = info[l].offset;
+        }
+    }
+    counts[0] = tot[0];
+    counts[1] = slab_total;
+    counts[2] = copy_total;
+    if (slab_total > slab_capacity || copy_total > copy_capacity)
+        return efail(DISCO_ELIMIT, "slab or copy capacity too small (counts hold the sizes needed)");
+    if (tot[1] > member_cap)
+        return efail(DISCO_ELIMIT, "more atoms in slabs than the member list holds");
     return DISCO_OK;
 }
 
@@ -562,15 +797,24 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     if (!(box[0] > 0.) || !(box[1] > 0.) || !(box[2] > 0.)) return efail(DISCO_EINVAL, "box lengths must be positive");
     int dcount = 0;
     if (cudaGetDeviceCount(&dcount) != cudaSuccess || dcount == 0) return efail(DISCO_ENODEV, "no CUDA device");
-    std::vector<SlabLoopDev> act;
-    std::vector<int> act_index;
-    int st = prepare_loops(loops, nloops, box, info, act, act_index);
-    if (st) return st;
-    const int nl = (int)act.size();
-    const int C = nl + 1;
-    const int64_t ntiles = (n + kSlabTile - 1) / kSlabTile;
+    int act_index[kMaxSlabLoops];
+    int nl = 0;
+    for (int l = 0; l < nloops; ++l) {                  // count the active loops first (sizes)
+        disco_slab_info in;
+        SlabHead h;
+        SlabLoopDev d;
+        bool active = false;
+        const int st0 = slab_loop_record(loops[l], box, in, h, d, active);
+        if (st0) return st0;
+        nl += active;
+    }
+    if (nl > kMaxSlabLoops) return efail(DISCO_ELIMIT, "more than 64 prismatic loops in one call");
+    const int C = 2 + 2 * nl;
+    const int64_t ntiles = (n + kMatterTile - 1) / kMatterTile;
+    const int64_t member_cap = std::max<int64_t>(1, std::min<int64_t>(n, slab_capacity));
+    const int64_t scap = std::max<int64_t>(1, slab_capacity), ccap = std::max<int64_t>(1, copy_capacity);
 
-    DevBuf dxyz, dout, didx, dloops, dcnt, doff, dtot, dslab, dside, dcop;
+    DevBuf dxyz, dout, didx, dloops, dstat, dexcl, dmem, dtot, dslab, dside, dcop;
     const size_t nb = (size_t)n * sizeof(double);
     cudaError_t e = cudaSuccess;
     if (n > 0) {
@@ -578,92 +822,62 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
         if (e == cudaSuccess) e = cudaMalloc(&dout.p, 3 * nb);
         if (e == cudaSuccess) e = cudaMalloc(&didx.p, (size_t)n * sizeof(int32_t));
     }
-    if (e == cudaSuccess) e = cudaMalloc(&dloops.p, std::max<size_t>(1, act.size()) * sizeof(SlabLoopDev));
-    if (e == cudaSuccess) e = cudaMalloc(&dcnt.p, std::max<int64_t>(1, ntiles * C) * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&doff.p, std::max<int64_t>(1, ntiles * C) * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&dtot.p, (size_t)(2 * C + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dloops.p, sizeof(LoopStage));
+    if (e == cudaSuccess) e = cudaMalloc(&dstat.p, status_bytes(ntiles, C));
+    if (e == cudaSuccess) e = cudaMalloc(&dexcl.p, std::max<int64_t>(1, ntiles * C) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dmem.p, (size_t)member_cap * sizeof(MemberRec));
+    if (e == cudaSuccess) e = cudaMalloc(&dtot.p, (size_t)(C + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dslab.p, (size_t)scap * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dside.p, (size_t)scap);
+    if (e == cudaSuccess) e = cudaMalloc(&dcop.p, (size_t)ccap * sizeof(disco_copy));
     if (e != cudaSuccess) return cfail(e, "prismatic allocation");
     if (n > 0) {
         e = cudaMemcpy(dxyz.as<double>(), x, nb, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(dxyz.as<double>() + n, y, nb, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(dxyz.as<double>() + 2 * n, z, nb, cudaMemcpyHostToDevice);
     }
-    if (e == cudaSuccess && nl > 0)
-        e = cudaMemcpy(dloops.p, act.data(), act.size() * sizeof(SlabLoopDev), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(dtot.p, 0, (size_t)(2 * C + 1) * sizeof(int64_t));
     if (e != cudaSuccess) return cfail(e, "prismatic upload");
+    int st = stage_loops(loops, nloops, box, info, act_index, nl, dloops.as<unsigned char>(), nullptr);
+    if (st) return st;
 
-    SlabArgs a;
+    MatterArgs a;
     std::memset(&a, 0, sizeof(a));
     a.x = dxyz.as<double>(); a.y = a.x + n; a.z = a.x + 2 * n;
     a.n = n;
-    a.loops = dloops.as<SlabLoopDev>();
-    a.nl = nl;
     a.Lx = box[0]; a.Ly = box[1]; a.Lz = box[2];
     a.iLx = (float)(1.0 / box[0]); a.iLy = (float)(1.0 / box[1]); a.iLz = (float)(1.0 / box[2]);
-    a.tile_counts = dcnt.as<int32_t>();
-    a.tile_offsets = doff.as<int32_t>();
-    a.totals = dtot.as<int64_t>();
     a.xo = dout.as<double>(); a.yo = a.xo + n; a.zo = a.xo + 2 * n;
     a.new_index = didx.as<int32_t>();
-    const size_t smem = act.size() * sizeof(SlabLoopDev);
-    if (smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(slab_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(slab_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return cfail(e, "prismatic smem");
-    }
-    if (ntiles > 0) slab_count_kernel<<<slab_grid(ntiles), kSlabThreads, smem>>>(a);
-    slab_scan_kernel<<<(unsigned)C, 1024>>>(a, ntiles);
-    std::vector<int64_t> tot(2 * C + 1, 0);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpy(tot.data(), dtot.p, tot.size() * sizeof(int64_t), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cfail(e, "prismatic count/scan");
-    int64_t slab_total = 0, inter_total = 0;
-    for (int l = 0; l < nl; ++l) {
-        slab_total += tot[1 + l];
-        if (act[l].type == DISCO_MATTER_INTERSTITIAL) inter_total += tot[1 + l];
-    }
-    e = cudaMalloc(&dslab.p, std::max<int64_t>(1, slab_total) * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&dside.p, std::max<int64_t>(1, slab_total));
-    if (e == cudaSuccess) e = cudaMalloc(&dcop.p, std::max<int64_t>(1, inter_total) * sizeof(disco_copy));
-    if (e != cudaSuccess) return cfail(e, "prismatic slab buffers");
     a.slab_atoms = dslab.as<int32_t>();
     a.slab_side = dside.as<int8_t>();
-    if (ntiles > 0) slab_scatter_kernel<<<slab_grid(ntiles), kSlabThreads, smem>>>(a);
-    slab_copies_kernel<<<1, 1024>>>(a, dcop.as<disco_copy>(), inter_total);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpy(tot.data(), dtot.p, tot.size() * sizeof(int64_t), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cfail(e, "prismatic scatter");
-    const int64_t k = tot[0];
-    counts[0] = k;
-    counts[1] = slab_total;
-    counts[2] = tot[2 * C - 1];
-    for (int q = 0; q < nl; ++q) {
-        disco_slab_info& in = info[act_index[q]];
-        in.offset = tot[C + q];
-        in.count = tot[1 + q];
-    }
-    // offsets of inactive loops: where the next active loop starts (empty ranges)
-    {
-        int64_t next = slab_total;
-        for (int l = nloops - 1; l >= 0; --l) {
-            if (info[l].type == DISCO_MATTER_NONE) info[l].offset = next;
-            else next = info[l].offset;
-        }
-    }
-    if (counts[1] > slab_capacity || counts[2] > copy_capacity)
-        return efail(DISCO_ELIMIT, "slab or copy capacity too small (counts hold the sizes needed)");
+    a.slab_cap = slab_capacity;
+    a.copies = dcop.as<disco_copy>();
+    a.copy_cap = copy_capacity;
+    MatterScratch m;
+    m.loops = dloops.as<unsigned char>();
+    m.status = dstat.as<unsigned char>();
+    m.tile_excl = dexcl.as<int32_t>();
+    m.members = dmem.as<MemberRec>();
+    m.member_cap = member_cap;
+    m.totals = dtot.as<int64_t>();
+    st = matter_queue(a, m, nl, ntiles, nullptr);
+    if (st) return st;
+    int64_t tot[kMaxCats + 1];
+    e = cudaMemcpy(tot, m.totals, (size_t)(C + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cfail(e, "prismatic totals");
+    st = matter_finish(tot, nl, act_index, nloops, info, slab_capacity, copy_capacity, member_cap, counts);
+    if (st) return st;
+    const int64_t k = counts[0];
     if (n > 0) {
         e = cudaMemcpy(new_index, didx.p, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost);
         if (e == cudaSuccess && k > 0) e = cudaMemcpy(x_out, a.xo, (size_t)k * sizeof(double), cudaMemcpyDeviceToHost);
         if (e == cudaSuccess && k > 0) e = cudaMemcpy(y_out, a.yo, (size_t)k * sizeof(double), cudaMemcpyDeviceToHost);
         if (e == cudaSuccess && k > 0) e = cudaMemcpy(z_out, a.zo, (size_t)k * sizeof(double), cudaMemcpyDeviceToHost);
     }
-    if (e == cudaSuccess && slab_total > 0)
-        e = cudaMemcpy(slab_atoms, dslab.p, (size_t)slab_total * sizeof(int32_t), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && slab_total > 0)
-        e = cudaMemcpy(slab_side, dside.p, (size_t)slab_total, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && counts[1] > 0)
+        e = cudaMemcpy(slab_atoms, dslab.p, (size_t)counts[1] * sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && counts[1] > 0)
+        e = cudaMemcpy(slab_side, dside.p, (size_t)counts[1], cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && counts[2] > 0)
         e = cudaMemcpy(copies, dcop.p, (size_t)counts[2] * sizeof(disco_copy), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cfail(e, "prismatic download");
@@ -742,20 +956,26 @@ int disco_b200_finalize_resident(const double* x, const double* y, const double*
 // memory pool, a code that may not synchronise the device the way cudaFree
 // does, a process with a fixed memory budget) cannot let the library call
 // cudaMalloc.  disco_b200_prismatic_noalloc takes device inputs and outputs
-// from the caller and keeps its scratch (active loop table, per-tile counts
-// and offsets, totals) in the file-scope array below: 1.25 MiB that every GPU
-// loading this library holds until the process exits.
+// from the caller and keeps its scratch (loop table, look-back words, per-tile
+// prefixes, member records, totals) in the file-scope array below: 3.25 MiB
+// that every GPU loading this library holds until the process exits.
 
 namespace {
 
 constexpr int64_t kNoAllocMaxAtoms = int64_t(1) << 22;                  // 4 194 304 atoms
-constexpr int64_t kNoAllocMaxTiles = kNoAllocMaxAtoms / disco::kSlabTile;
-constexpr size_t kNoAllocLoopBytes = disco::kMaxSlabLoops * sizeof(disco::SlabLoopDev);
-constexpr size_t kNoAllocTotalsBytes = (2 * (disco::kMaxSlabLoops + 1) + 1) * sizeof(int64_t);
-constexpr size_t kNoAllocTileBytes = kNoAllocMaxTiles * (disco::kMaxSlabLoops + 1) * sizeof(int32_t);
-constexpr size_t kNoAllocScratchBytes = 1280 * 1024;
-static_assert(((kNoAllocLoopBytes + 255) & ~size_t(255)) + ((kNoAllocTotalsBytes + 255) & ~size_t(255)) +
-                  2 * kNoAllocTileBytes <= kNoAllocScratchBytes,
+constexpr int64_t kNoAllocMaxTiles = kNoAllocMaxAtoms / disco::kMatterTile;
+constexpr int64_t kNoAllocMaxMembers = int64_t(1) << 16;                // atoms in slabs
+constexpr size_t align256c(size_t v) { return (v + 255) & ~size_t(255); }
+constexpr size_t kNoAllocLoopOff = 0;
+constexpr size_t kNoAllocStatusOff = kNoAllocLoopOff + align256c(sizeof(LoopStage));
+constexpr size_t kNoAllocExclOff =
+    kNoAllocStatusOff + align256c(16 + (size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(unsigned long long));
+constexpr size_t kNoAllocMemberOff =
+    kNoAllocExclOff + align256c((size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(int32_t));
+constexpr size_t kNoAllocTotalsOff =
+    kNoAllocMemberOff + align256c((size_t)kNoAllocMaxMembers * sizeof(disco::MemberRec));
+constexpr size_t kNoAllocScratchBytes = 3328 * 1024;
+static_assert(kNoAllocTotalsOff + (disco::kMaxCats + 1) * sizeof(int64_t) <= kNoAllocScratchBytes,
               "no-alloc scratch layout");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -763,28 +983,62 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_addr[kMaxDevices] = {};
+unsigned long long g_noalloc_ctx[kMaxDevices] = {};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// Unique identifier of the calling thread's current context (the driver's
+// cuCtxGetId, reached through the runtime without linking libcuda), 0 when
+// it cannot be read.
+unsigned long long current_context_id()
+{
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<CtxGetIdFn>(f);
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_current && get_id && get_current(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
 
 // Device address of g_noalloc_scratch on the current device.  In host code the
 // array's name is a host-side stand-in, not a device address: the address is
-// looked up once per device with that device current and cached.
+// looked up with that device current and cached with the identifier of the
+// context it belongs to; a new context on that device (after a device reset,
+// which reloads the module) gets a fresh lookup.
 int noalloc_scratch(unsigned char** out)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cfail(e, "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDevices) return efail(DISCO_ELIMIT, "device ordinal above 63");
+    // make the primary context current before its identifier is read
+    e = cudaFree(nullptr);
+    if (e != cudaSuccess) return cfail(e, "device context");
+    const unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
+    if (!g_noalloc_addr[dev] || ctx == 0 || ctx != g_noalloc_ctx[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) return cfail(e, "cudaGetSymbolAddress of the scratch array");
         g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+        g_noalloc_ctx[dev] = ctx;
     }
     *out = g_noalloc_addr[dev];
     return DISCO_OK;
 }
-
-size_t align256(size_t v) { return (v + 255) & ~size_t(255); }
 
 } // namespace
 
@@ -807,97 +1061,52 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     if (!(box[0] > 0.) || !(box[1] > 0.) || !(box[2] > 0.)) return efail(DISCO_EINVAL, "box lengths must be positive");
     if (n > kNoAllocMaxAtoms)
         return efail(DISCO_ELIMIT, "disco_b200_prismatic_noalloc takes at most 4194304 atoms (its scratch array is fixed)");
+    int dcount = 0;
+    if (cudaGetDeviceCount(&dcount) != cudaSuccess || dcount == 0) return efail(DISCO_ENODEV, "no CUDA device");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* base = nullptr;
     int st = noalloc_scratch(&base);
     if (st) return st;
-    SlabLoopDev* d_loops = reinterpret_cast<SlabLoopDev*>(base);
-    int64_t* d_tot = reinterpret_cast<int64_t*>(base + align256(kNoAllocLoopBytes));
-    int32_t* d_cnt = reinterpret_cast<int32_t*>(base + align256(kNoAllocLoopBytes) + align256(kNoAllocTotalsBytes));
-    int32_t* d_off = d_cnt + kNoAllocMaxTiles * (kMaxSlabLoops + 1);
 
-    // active loops, one record at a time from the stack (no host allocation)
-    int nl = 0;
     int act_index[kMaxSlabLoops];
-    cudaError_t e = cudaSuccess;
-    for (int l = 0; l < nloops; ++l) {
-        SlabLoopDev d;
-        bool active = false;
-        st = slab_loop_record(loops[l], l, box, info[l], d, active);
-        if (st) return st;
-        if (!active) continue;
-        if (nl >= kMaxSlabLoops) return efail(DISCO_ELIMIT, "more than 64 prismatic loops in one call");
-        e = cudaMemcpyAsync(d_loops + nl, &d, sizeof(d), cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) return cfail(e, "loop table upload");
-        act_index[nl++] = l;
-    }
-    const int C = nl + 1;
-    const int64_t ntiles = (n + kSlabTile - 1) / kSlabTile;
-    // the array keeps the previous call's contents: the totals must start at zero
-    e = cudaMemsetAsync(d_tot, 0, kNoAllocTotalsBytes, s);
-    if (e != cudaSuccess) return cfail(e, "totals reset");
+    int nl = 0;
+    st = stage_loops(loops, nloops, box, info, act_index, nl, base + kNoAllocLoopOff, s);
+    if (st) return st;
+    const int C = 2 + 2 * nl;
+    const int64_t ntiles = (n + kMatterTile - 1) / kMatterTile;
+    const int64_t member_cap = std::min<int64_t>(kNoAllocMaxMembers, std::max<int64_t>(0, slab_capacity));
 
-    SlabArgs a;
+    MatterArgs a;
     std::memset(&a, 0, sizeof(a));
     a.x = x; a.y = y; a.z = z;
     a.n = n;
-    a.loops = d_loops;
-    a.nl = nl;
     a.Lx = box[0]; a.Ly = box[1]; a.Lz = box[2];
     a.iLx = (float)(1.0 / box[0]); a.iLy = (float)(1.0 / box[1]); a.iLz = (float)(1.0 / box[2]);
-    a.tile_counts = d_cnt;
-    a.tile_offsets = d_off;
-    a.totals = d_tot;
     a.xo = x_out; a.yo = y_out; a.zo = z_out;
     a.new_index = new_index;
     a.slab_atoms = slab_atoms;
     a.slab_side = slab_side;
-    const size_t smem = (size_t)nl * sizeof(SlabLoopDev);
-    if (smem > 48 * 1024) {
-        e = cudaFuncSetAttribute(slab_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(slab_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return cfail(e, "prismatic smem");
-    }
-    if (ntiles > 0) slab_count_kernel<<<slab_grid(ntiles), kSlabThreads, smem, s>>>(a);
-    slab_scan_kernel<<<(unsigned)C, 1024, 0, s>>>(a, ntiles);
-    int64_t tot[2 * (kMaxSlabLoops + 1) + 1];
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(tot, d_tot, (size_t)(2 * C) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    a.slab_cap = slab_capacity;
+    a.copies = copies;
+    a.copy_cap = copy_capacity;
+    MatterScratch m;
+    m.loops = base + kNoAllocLoopOff;
+    m.status = base + kNoAllocStatusOff;
+    m.tile_excl = reinterpret_cast<int32_t*>(base + kNoAllocExclOff);
+    m.members = reinterpret_cast<MemberRec*>(base + kNoAllocMemberOff);
+    m.member_cap = member_cap;
+    m.totals = reinterpret_cast<int64_t*>(base + kNoAllocTotalsOff);
+    st = matter_queue(a, m, nl, ntiles, s);
+    if (st) return st;
+    int64_t tot[kMaxCats + 1];
+    cudaError_t e = cudaMemcpyAsync(tot, m.totals, (size_t)(C + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cfail(e, "prismatic count/scan");
-    int64_t slab_total = 0, inter_total = 0;
-    for (int q = 0; q < nl; ++q) {
-        slab_total += tot[1 + q];
-        // copies can only come from interstitial slabs
-        disco_slab_info& in = info[act_index[q]];
-        if (in.type == DISCO_MATTER_INTERSTITIAL) inter_total += tot[1 + q];
-        in.offset = tot[C + q];
-        in.count = tot[1 + q];
-    }
-    {
-        int64_t next = slab_total;
-        for (int l = nloops - 1; l >= 0; --l) {
-            if (info[l].type == DISCO_MATTER_NONE) info[l].offset = next;
-            else next = info[l].offset;
-        }
-    }
-    counts[0] = tot[0];
-    counts[1] = slab_total;
-    counts[2] = inter_total;         // upper bound until the copies pass has run
-    if (slab_total > slab_capacity)
-        return efail(DISCO_ELIMIT, "slab capacity too small (counts[1] holds the size needed)");
-    if (ntiles > 0) slab_scatter_kernel<<<slab_grid(ntiles), kSlabThreads, smem, s>>>(a);
-    slab_copies_kernel<<<1, 1024, 0, s>>>(a, copies, copy_capacity);
-    e = cudaGetLastError();
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(&tot[2 * C - 1], d_tot + (2 * C - 1), sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cfail(e, "prismatic scatter");
-    counts[2] = tot[2 * C - 1];
-    if (counts[2] > copy_capacity)
-        return efail(DISCO_ELIMIT, "copy capacity too small (counts[2] holds the size needed)");
-    return DISCO_OK;
+    if (e != cudaSuccess) return cfail(e, "prismatic totals");
+    st = matter_finish(tot, nl, act_index, nloops, info, slab_capacity, copy_capacity, member_cap, counts);
+    if (st == DISCO_ELIMIT && tot[1] > member_cap && counts[1] <= slab_capacity && counts[2] <= copy_capacity)
+        return efail(DISCO_ELIMIT, "disco_b200_prismatic_noalloc takes at most 65536 atoms in slabs "
+                                   "(its scratch array is fixed)");
+    return st;
 }
 
 } // extern "C"

@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import geometry as G
+from . import geometry as _G
 
 # {111} normals and the <110> directions in each of those planes
 _N111 = [(1, 1, 1), (-1, 1, 1), (1, -1, 1), (1, 1, -1)]
@@ -50,7 +50,7 @@ class Workload:
     images: int
     nu: float
     method: str                      # "line" or "loopons"
-    lattice: int = G.BCC
+    lattice: int = _G.BCC
     a0: float = 0.0
     cells: tuple = (0, 0, 0)
     slab_loops: list = field(default_factory=list)
@@ -73,9 +73,10 @@ class Workload:
         return w
 
 
-def quadrupole(cells=40, a0=2.855, radius=30.0, eps=0.0365, nu=0.29, images=1, da=1.0):
+def quadrupole(cells=40, a0=2.855, radius=30.0, eps=0.0365, nu=0.29, images=1, da=1.0, geom=None):
     """Four circular shear loops forming a quadrupole (the pattern of the
     reference's Examples/quadrupole_circle.yaml), line method."""
+    G = geom or _G
     L = cells * a0
     q = L / 4.0
     specs = [((-q, -q, 0.0), (1, -1, -1), (1, 1, 0)),
@@ -93,7 +94,7 @@ def quadrupole(cells=40, a0=2.855, radius=30.0, eps=0.0365, nu=0.29, images=1, d
                     (cells, cells, cells), geom=geom)
 
 
-def _fcc_glide_loop(rng, kind, cells, a0, da, chords):
+def _fcc_glide_loop(rng, kind, cells, a0, da, chords, G):
     """One glide loop of the fcc_random distribution: a random {111} plane, b =
     a0/2<110> in it, centre uniform in the box (snapped to a mid-plane)."""
     L = cells * a0
@@ -118,32 +119,34 @@ def _fcc_glide_loop(rng, kind, cells, a0, da, chords):
 
 
 def fcc_random(cells=150, a0=3.615, nu=0.34, images=2, seed=2, n_circles=32, n_hex=16, n_rect=16,
-               chords=48, da=1.0):
+               chords=48, da=1.0, geom=None):
     """64 random shear loops in an FCC box, line method."""
+    G = geom or _G
     rng = np.random.default_rng(seed)
     L = cells * a0
     x, y, z = G.lattice(G.FCC, cells, cells, cells, a0)
     loops, geom = [], []
     kinds = ["circle"] * n_circles + ["hexagon"] * n_hex + ["rectangle"] * n_rect
     for kind in kinds:
-        lp, ld = _fcc_glide_loop(rng, kind, cells, a0, da, chords)
+        lp, ld = _fcc_glide_loop(rng, kind, cells, a0, da, chords, G)
         geom.append(lp)
         loops.append(ld)
     return Workload("fcc_random", x, y, z, loops, (L, L, L), images, nu, "line", G.FCC, a0,
                     (cells, cells, cells), geom=geom)
 
 
-def fcc_random_loops(count, seed, cells=150, a0=3.615, chords=48, da=1.0):
+def fcc_random_loops(count, seed, cells=150, a0=3.615, chords=48, da=1.0, geom=None):
     """`count` loops drawn from the fcc_random distribution (kinds in its
     proportions: half circles, a quarter hexagons, a quarter rectangles)."""
     rng = np.random.default_rng(seed)
     kinds = rng.choice(["circle", "circle", "hexagon", "rectangle"], size=count)
-    return [_fcc_glide_loop(rng, k, cells, a0, da, chords)[1] for k in kinds]
+    return [_fcc_glide_loop(rng, k, cells, a0, da, chords, geom or _G)[1] for k in kinds]
 
 
 def bcc_prismatic(cells=60, a0=3.165, nu=0.28, images=1, seed=3, n_inter=8, n_vac=8, da=1.0,
-                  rmin=20.0, rmax=50.0):
+                  rmin=20.0, rmax=50.0, geom=None):
     """16 prismatic circular loops (loopon method) with their slab loops."""
+    G = geom or _G
     rng = np.random.default_rng(seed)
     L = cells * a0
     x, y, z = G.lattice(G.BCC, cells, cells, cells, a0)
@@ -164,6 +167,45 @@ def bcc_prismatic(cells=60, a0=3.165, nu=0.28, images=1, seed=3, n_inter=8, n_va
                     (cells, cells, cells), slab_loops=slabs, geom=geom)
 
 
+def on_plane(cells=12, a0=2.855, nu=0.35, images=1, radius=8.8, eps=0.0365, geom=None):
+    """Loops whose planes pass through lattice sites: each centre is an atom
+    (not snapped to a mid-plane), so every loop has atoms exactly on its plane
+    inside and outside the contour, one at its centre, and some on the rays
+    from the centre to its vertices.  BCC box, line method; circles on (001),
+    (110), (1-10), (111) and (112), a hexagon on (1-10), a rectangle on (001).
+    The reference's cut surface decides which side such an atom is on by the
+    rounding of its solid-angle arithmetic (Code/barnett.hpp:69-72)."""
+    G = geom or _G
+    L = cells * a0
+    x, y, z = G.lattice(G.BCC, cells, cells, cells, a0)
+    q = L / 4.0
+    specs = [("circle", (0, 0, 1), (1, 0, 0), (-q, -q, -q)),
+             ("circle", (1, 1, 0), (1, -1, 1), (q, -q, -q)),
+             ("circle", (1, -1, 0), (1, 1, 1), (-q, q, -q)),
+             ("circle", (1, 1, 1), (1, 1, 1), (q, q, -q)),
+             ("circle", (1, 1, 2), (1, 1, -1), (-q, -q, q)),
+             ("hexagon", (1, -1, 0), (1, 1, -1), (q, -q, q)),
+             ("rectangle", (0, 0, 1), (0, 1, 0), (-q, q, q))]
+    pos = np.stack([x, y, z], 1)
+    loops, geom = [], []
+    for kind, n, m, target in specs:
+        i = int(np.argmin(((pos - np.array(target)) ** 2).sum(1)))
+        c = (float(x[i]), float(y[i]), float(z[i]))
+        if kind == "circle":
+            lp = G.Loop.circle(1.0, radius, c, m, n, a0)
+            P = lp.polyline(eps)
+        elif kind == "hexagon":
+            lp = G.Loop.polygon(1.0, G.regular_polygon(6, radius, m, n), 0.0, c, m, n, a0)
+            P = lp.polyline(0.01)
+        else:
+            lp = G.Loop.rectangle(1.0, radius, 0.6 * radius, 0.0, c, m, n, a0)
+            P = lp.polyline(0.01)
+        geom.append(lp)
+        loops.append(lp.line_data(vertices=P))
+    return Workload("on_plane", x, y, z, loops, (L, L, L), images, nu, "line", G.BCC, a0,
+                    (cells, cells, cells), geom=geom)
+
+
 _N110 = [(1, 1, 0), (1, -1, 0), (1, 0, 1), (1, 0, -1), (0, 1, 1), (0, 1, -1)]
 _N112 = [(1, 1, 2), (1, 1, -2), (1, -1, 2), (-1, 1, 2), (1, 2, 1), (1, 2, -1), (1, -2, 1), (-1, 2, 1),
          (2, 1, 1), (2, 1, -1), (2, -1, 1), (-2, 1, 1)]
@@ -171,12 +213,13 @@ _B111 = [(1, 1, 1), (1, 1, -1), (1, -1, 1), (-1, 1, 1)]
 
 
 def batch(nsamples=256, a0=2.855, edge=(20, 80), nloops=(1, 32), radius=(8.0, 40.0),
-          segments=(16, 128), images=(1, 3), nu=0.29, seed=4, da=1.0):
+          segments=(16, 128), images=(1, 3), nu=0.29, seed=4, da=1.0, geom=None):
     """Many independent BCC samples for the batched form: box edges uniform
     integers in `edge` (cells, independent per axis), 1-32 glide loops each
     (circles of `segments` chords or regular hexagons, radius in `radius`), on
     random {110}<111> or {112}<111> systems with a random sign of b, centres
     uniform, images +-U{images}."""
+    G = geom or _G
     rng = np.random.default_rng(seed)
     out = []
     for s in range(nsamples):

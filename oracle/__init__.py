@@ -16,6 +16,7 @@ ORACLE_SO = os.path.join(HERE, "_build", "libdisco_oracle.so")
 ORACLE_NOFMA_SO = os.path.join(HERE, "_build", "libdisco_oracle_nofma.so")
 REF_SO = os.path.join(HERE, "_ref", "libdisco_ref.so")
 REF_NOFMA_SO = os.path.join(HERE, "_ref", "libdisco_ref_nofma.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libdisco_ref_cuda.so")
 
 _libs = {}
 
@@ -31,7 +32,12 @@ def _load(path):
             raise ImportError(f"oracle library missing: {path} (run oracle/build_oracle.py)")
         lib = ctypes.CDLL(path)
         C = _capi()
-        if "libdisco_ref" in path:
+        if "libdisco_ref_cuda" in path:
+            lib.ref_gpu_available.restype = c_int
+            lib.ref_kroupa_gpu.restype = c_int
+            lib.ref_kroupa_gpu.argtypes = [POINTER(C.DiscoAtoms), POINTER(C.DiscoLoop), c_int,
+                                           POINTER(c_double), c_int, c_void_p]
+        elif "libdisco_ref" in path:
             lib.ref_kroupa_cpu.restype = c_int
             lib.ref_kroupa_cpu.argtypes = [POINTER(C.DiscoAtoms), POINTER(C.DiscoLoop), c_int,
                                            POINTER(c_double), c_void_p]
@@ -110,6 +116,10 @@ def have_ref():
     return os.path.exists(REF_SO)
 
 
+def have_ref_cuda():
+    return os.path.exists(REF_CUDA_SO)
+
+
 def _box(box):
     return (c_double * 3)(*[float(v) for v in box])
 
@@ -152,6 +162,20 @@ def ref_displace(x, y, z, loops, box, loop_sec=None, nofma=False):
     if loop_sec is not None:
         loop_sec[:] = ls[:len(loops)]
     return u
+
+
+def ref_displace_gpu(x, y, z, loops, box, fp32=False):
+    """The reference's own kroupaGPU (Code/backend_cuda.cu, built for sm_100a;
+    images +-1, nu 0.35): (ux, uy, uz) and its (upload, kernels, download)
+    seconds as it measures them."""
+    from disco_b200.backend import loop_array
+    lib = _load(REF_CUDA_SO)
+    a, keep_x, u = _atoms(x, y, z)
+    arr, keep = loop_array(loops)
+    t = np.zeros(3)
+    st = lib.ref_kroupa_gpu(ctypes.byref(a), arr, len(loops), _box(box), int(fp32), t.ctypes.data)
+    assert st == 0
+    return u, t
 
 
 def barnett_loop(p, V, c, b, nu):
@@ -353,3 +377,77 @@ def ref_prismatic(ref_loops, spacing, x, y, z, box, apply=None, frank=None, a0=0
         return lib.ref_prismatic_step(handles, sp.ctypes.data, ap.ctypes.data, fr.ctypes.data, a0,
                                       nl, x_, y_, z_, n, box_, *rest)
     return _prismatic_call(fn, x, y, z, ref_loops, box)
+
+
+class RefGeometry:
+    """The geometry calls of disco_b200.workloads answered by the reference's
+    own code (oracle/_ref: generateLattice, snapToMidPlane, regularPolygon and
+    the loop class), so that a workload can be built without this library's
+    geometry: workloads.fcc_random(geom=RefGeometry) and so on.  LoopData is
+    filled as Code/main.cpp:689-711 fills it."""
+    BCC, FCC = 0, 1
+
+    @staticmethod
+    def lattice(kind, nx, ny, nz, a0):
+        return ref_lattice(kind, nx, ny, nz, a0)
+
+    @staticmethod
+    def snap(center, n, a0, nx, ny, nz, kind):
+        return ref_snap(center, n, a0, nx, ny, nz, kind)
+
+    @staticmethod
+    def regular_polygon(sides, R, m, n, vertex_dir=None):
+        return ref_regular_polygon(sides, R, m, n, vertex_dir)
+
+    @staticmethod
+    def circle_eps_for_chords(radius, chords):
+        lo = 1.0 - np.cos(np.pi / chords)
+        hi = 1.0 - np.cos(np.pi / (chords - 1))
+        return radius * 0.5 * (lo + hi)
+
+    class Loop:
+        def __init__(self, ref):
+            self.ref = ref
+            self._info = ref.info()
+
+        @staticmethod
+        def circle(da, radius, c, m, n, a0):
+            return RefGeometry.Loop(RefLoop(0, da, c, m, n, a0, radius=radius))
+
+        @staticmethod
+        def rectangle(da, half_m, half_p, corner_r, c, m, n, a0, side=None):
+            return RefGeometry.Loop(RefLoop(1, da, c, m, n, a0, half_m=half_m, half_p=half_p,
+                                            corner_r=corner_r, side=side))
+
+        @staticmethod
+        def polygon(da, verts, corner_r, c, m, n, a0, axis=None):
+            return RefGeometry.Loop(RefLoop(3, da, c, m, n, a0, corner_r=corner_r, side=axis,
+                                            verts=np.asarray(verts, dtype=np.float64).reshape(-1, 3)))
+
+        @property
+        def center(self):
+            return np.array(self._info["c"])
+
+        def polyline(self, eps):
+            return self.ref.polyline(eps)
+
+        def _phys(self, dS):
+            from disco_b200.backend import LoopPhys
+            i = self._info
+            return LoopPhys(*i["b"], *i["m"], *i["n"], dS)
+
+        def line_data(self, eps=None, vertices=None):
+            from disco_b200.backend import LoopData
+            P = vertices if vertices is not None else self.polyline(eps)
+            _, dS = self.ref.loopons()
+            c = self.center
+            return LoopData(phys=self._phys(dS), line=True, vx=P[:, 0].copy(), vy=P[:, 1].copy(),
+                            vz=P[:, 2].copy(), cx=c[0], cy=c[1], cz=c[2])
+
+        def loopon_data(self):
+            from disco_b200.backend import LoopData
+            L, dS = self.ref.loopons()
+            return LoopData(x=L[:, 0].copy(), y=L[:, 1].copy(), z=L[:, 2].copy(), phys=self._phys(dS))
+
+        def slab_loop(self, spacing, apply=True, frank=False, a0=0.0):
+            return None          # the reference's matter step takes the loop object itself

@@ -9,6 +9,10 @@ loops) or the output of a reference function on that input:
               4 circular glide loops in a 10^3-cell BCC box, nu 0.35, images +-1
   loopon_*    kroupaCPU loopon branch (Code/backend_cpu.cpp:64-96), 16 prismatic
               circles in a 10^3-cell BCC box
+  plane_*     kroupaCPU line branch on loops whose planes pass through lattice
+              sites (workloads.on_plane: atoms exactly on a loop's plane,
+              inside and outside the contour, at its centre and on fan edges),
+              nu 0.35, images +-1
   slab_*      prismaticSlab (Code/prismatic.cpp:36-74) driven as
               Code/main.cpp:586-687 drives it, 16 prismatic circles, 12^3 cells
 Outputs are stored for both builds of the reference (default flags and
@@ -39,7 +43,8 @@ def _loops_arrays(loops, prefix, d):
 
 def main():
     from oracle import build_oracle
-    build_oracle.build(verbose=False)
+    import __graft_entry__ as G
+    build_oracle.build(verbose=False, reference=G.REFERENCE_CODE)
     import oracle as O
     from disco_b200 import workloads as W
     from disco_b200 import _capi as C
@@ -59,6 +64,13 @@ def main():
     _loops_arrays(w.loops, "loopon", d)
     d["loopon_u"] = np.stack(O.ref_displace(w.x, w.y, w.z, w.loops, w.box), 1)
     d["loopon_u_nofma"] = np.stack(O.ref_displace(w.x, w.y, w.z, w.loops, w.box, nofma=True), 1)
+
+    w = W.on_plane()
+    d["plane_box"] = np.array(w.box)
+    d["plane_xyz"] = np.stack([w.x, w.y, w.z], 1)
+    _loops_arrays(w.loops, "plane", d)
+    d["plane_u"] = np.stack(O.ref_displace(w.x, w.y, w.z, w.loops, w.box), 1)
+    d["plane_u_nofma"] = np.stack(O.ref_displace(w.x, w.y, w.z, w.loops, w.box, nofma=True), 1)
 
     w = W.bcc_prismatic(cells=12, rmin=4.0, rmax=9.0, seed=33)
     refl = [O.RefLoop(0, 1.0, g.center, g.m_in, g.n_in, w.a0, radius=g.g.radius)

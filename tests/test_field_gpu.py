@@ -190,3 +190,42 @@ def test_far_field_series_tiers_and_logarithm():
     w = W.Workload("tiers", pos[0], pos[1], pos[2], loops, box, 0, 0.34, "line")
     got, ref = _gpu(w), _oracle(w)
     assert np.abs(got - ref).max() <= TOL
+
+
+def test_atoms_on_loop_planes_match_the_reference():
+    """Atoms exactly on a loop's plane, inside and outside the contour, at the
+    fan apex and on fan edges (loops centred on lattice sites, not snapped to
+    mid-planes): which side of the cut such an atom takes is decided by the
+    rounding of the reference's per-triangle solid angle
+    (Code/barnett.hpp:69-72), and the kernel reproduces it.  Checked atom for
+    atom against the reference's own output (golden vectors of its
+    contract-off build, tests/golden/make_golden.py) and against the oracle at
+    another nu and image range."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "reference_vectors.npz"))
+    w = W.on_plane()
+    assert np.array_equal(np.stack([w.x, w.y, w.z], 1), g["plane_xyz"])
+    got = _gpu(w, images=1, nu=0.35)
+    assert np.isfinite(got).all()
+    assert np.abs(got - g["plane_u_nofma"]).max() <= TOL
+    ref = np.stack(O.displace(w.x, w.y, w.z, w.loops, w.box, images=2, nu=0.29, nofma=True), 1)
+    assert np.abs(_gpu(w, images=2, nu=0.29) - ref).max() <= TOL
+    if O.have_ref():
+        live = np.stack(O.ref_displace(w.x, w.y, w.z, w.loops, w.box, nofma=True), 1)
+        assert np.abs(got - live).max() <= TOL
+
+
+def test_atoms_on_loop_planes_fp32c_and_batched():
+    """The same on-plane atoms through the FP32 compensated form (its FP64
+    near-cut pass takes the reference's side of the cut) and the batched
+    form."""
+    from disco_b200 import _capi as C
+    from disco_b200.backend import GpuOptions
+    w = W.on_plane()
+    ref = np.stack(O.displace(w.x, w.y, w.z, w.loops, w.box, images=1, nu=0.35, nofma=True), 1)
+    a = AtomArrays.zeros_like_positions(w.x, w.y, w.z)
+    B.kroupa_gpu(a, w.loops, *w.box, GpuOptions(fp32=True), images=1, nu=0.35)
+    assert np.abs(np.stack([a.ux, a.uy, a.uz], 1) - ref).max() <= 2e-5
+    us, _ = B.batch_gpu([w, w], C.DISCO_FP64)
+    for u in us:
+        assert np.abs(np.stack(u, 1) - ref).max() <= TOL

@@ -95,3 +95,32 @@ def test_burgers_classes_match():
             nn = np.ascontiguousarray(n, dtype=np.float64)
             assert lib.ref_classify_burgers(lat, mm.ctypes.data, nn.ctypes.data) == \
                 G.classify_burgers(lat, m, n)
+
+
+@pytest.mark.parametrize("name", ["quadrupole", "fcc_random", "bcc_prismatic", "on_plane", "batch"])
+def test_workloads_built_by_the_reference_geometry_are_identical(name):
+    """The workloads built entirely by the reference's own geometry code
+    (oracle.RefGeometry: generateLattice, snapToMidPlane, regularPolygon, the
+    loop class) equal the ones this library builds, atom for atom and vertex
+    for vertex (the reference arm of the bench uses the former)."""
+    from disco_b200 import workloads as W
+    make = {"quadrupole": lambda g: [W.quadrupole(cells=10, radius=8.0, geom=g)],
+            "fcc_random": lambda g: [W.fcc_random(cells=12, n_circles=6, n_hex=3, n_rect=3, seed=11, geom=g)],
+            "bcc_prismatic": lambda g: [W.bcc_prismatic(cells=10, rmin=4.0, rmax=8.0, geom=g)],
+            "on_plane": lambda g: [W.on_plane(geom=g)],
+            "batch": lambda g: W.batch(nsamples=3, edge=(5, 8), nloops=(1, 4), radius=(4.0, 8.0), geom=g)}[name]
+    for a, b in zip(make(None), make(O.RefGeometry)):
+        for k in "xyz":
+            assert np.array_equal(getattr(a, k), getattr(b, k))
+        assert len(a.loops) == len(b.loops)
+        for la, lb in zip(a.loops, b.loops):
+            for k in ("vx", "vy", "vz", "x", "y", "z"):
+                va, vb = getattr(la, k, None), getattr(lb, k, None)
+                if va is not None or vb is not None:
+                    assert np.array_equal(np.asarray(va), np.asarray(vb)), k
+            assert (la.cx, la.cy, la.cz) == (lb.cx, lb.cy, lb.cz)
+            pa, pb = la.phys, lb.phys
+            assert [pa.bx, pa.by, pa.bz, pa.mx, pa.my, pa.mz, pa.nx, pa.ny, pa.nz] == \
+                [pb.bx, pb.by, pb.bz, pb.mx, pb.my, pb.mz, pb.nx, pb.ny, pb.nz]
+            if not la.line:
+                assert pa.dS == pb.dS

@@ -56,6 +56,42 @@ def test_oracle_matches_golden_vectors(prefix):
     assert np.abs(u - g[prefix + "_u"]).max() < 1e-13
 
 
+def _on_plane_atoms(g, prefix):
+    """Atoms exactly on some loop's plane (integer arithmetic on lattice
+    coordinates: 2 (p - c) / a0 is integral for BCC sites and centres)."""
+    xyz = g[prefix + "_xyz"]
+    a0 = g[prefix + "_box"][0] / 12
+    on = np.zeros(len(xyz), bool)
+    for c, ph in zip(g[prefix + "_c"], g[prefix + "_phys"]):
+        n = ph[6:9]
+        q = np.rint(2 * (xyz - c) / a0)
+        k = n / np.abs(n[np.abs(n) > 1e-12]).min()
+        on |= np.abs(q @ np.rint(k)) == 0
+    return on
+
+
+def test_oracle_on_plane_matches_golden_vectors():
+    """Atoms exactly on a loop's plane (inside the contour, outside it, at
+    the fan apex, on fan edges): the contract-off restatement reproduces the
+    contract-off reference bit for bit, so it takes the same side of the cut
+    for every such atom.  The reference's two builds disagree with each other
+    there, by a whole Burgers vector on some atoms: an FMA-contracted build
+    rounds the solid-angle triple product differently
+    (Code/barnett.hpp:69), so only the source's operation order, without
+    contraction, defines the convention."""
+    g = _golden()
+    xyz = g["plane_xyz"]
+    loops = _golden_loops(g, "plane")
+    u = np.stack(O.displace(xyz[:, 0], xyz[:, 1], xyz[:, 2], loops, g["plane_box"],
+                            images=1, nu=0.35, nofma=True), 1)
+    assert np.array_equal(u, g["plane_u_nofma"])
+    on = _on_plane_atoms(g, "plane")
+    d = np.abs(g["plane_u"] - g["plane_u_nofma"]).max(1)
+    assert (d > 1e-9).any() and not (d[~on] > 1e-9).any()
+    bmax = max(np.linalg.norm(ph[0:3] * ph[3:6]) for ph in g["plane_phys"])
+    assert d.max() <= 1.0001 * bmax
+
+
 def test_oracle_prismatic_matches_golden_vectors():
     g = _golden()
     raw = g["slab_loops"].tobytes()

@@ -81,6 +81,42 @@ def test_noalloc_rejects_sizes_beyond_its_array():
                                           p, p, 0, None, 0, counts, None)
     assert st == C.DISCO_ELIMIT
     assert b"4194304" in lib.disco_b200_last_error()
-    # too small a slab capacity: DISCO_ELIMIT with the size needed, nothing written
+    # too small a slab capacity: DISCO_ELIMIT with the size needed in counts[1]
     st, counts, *_ = _noalloc(lib, torch, w, 1, 1, torch.cuda.current_stream().cuda_stream)
     assert st == C.DISCO_ELIMIT and counts[1] > 1
+
+
+def test_noalloc_copy_capacity_too_small():
+    """Enough room for the slabs, room for one copy: DISCO_ELIMIT with the
+    number of copies needed in counts[2], the first copy written exactly and
+    nothing written past the capacity."""
+    torch = pytest.importorskip("torch")
+    lib = C.cuda_lib()
+    w = W.bcc_prismatic(cells=24, rmin=6.0, rmax=14.0)
+    ref = P.prismatic(w.x, w.y, w.z, w.slab_loops, w.box)
+    ns, nc = len(ref["slab_atoms"]), len(ref["copy_atom"])
+    assert nc > 1
+    n = w.n
+    pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
+    out = torch.empty((3, n), dtype=torch.float64, device="cuda")
+    new_index = torch.empty(n, dtype=torch.int32, device="cuda")
+    slab_atoms = torch.empty(ns + 100, dtype=torch.int32, device="cuda")
+    slab_side = torch.empty(ns + 100, dtype=torch.int8, device="cuda")
+    copies = torch.full((4, 4), 7.0, dtype=torch.float64, device="cuda")      # 4 entries, capacity 1
+    nl = len(w.slab_loops)
+    loops = (C.DiscoSlabLoop * nl)(*w.slab_loops)
+    info = (C.DiscoSlabInfo * nl)()
+    counts = (ctypes.c_int64 * 3)()
+    box = (ctypes.c_double * 3)(*w.box)
+    st = lib.disco_b200_prismatic_noalloc(
+        pos[0].data_ptr(), pos[1].data_ptr(), pos[2].data_ptr(), n, loops, nl, box,
+        out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), new_index.data_ptr(), info,
+        slab_atoms.data_ptr(), slab_side.data_ptr(), ns + 100, copies.data_ptr(), 1, counts,
+        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    torch.cuda.synchronize()
+    assert st == C.DISCO_ELIMIT
+    assert counts[2] == nc and counts[1] == ns
+    cp = copies.cpu().numpy()
+    assert int(cp[0:1, 0].view(np.int64)[0] & 0xFFFFFFFF) == int(ref["copy_atom"][0])
+    assert np.array_equal(cp[0, 1:], ref["copy_shift"][0])
+    assert (cp[1:] == 7.0).all()

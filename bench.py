@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--no-output", action="store_true", help="skip the output-writer measurement")
     p.add_argument("--no-forms", action="store_true",
                    help="default workload: skip the fp32c, learned and bcc_prismatic keys")
+    p.add_argument("--kernel-only", action="store_true",
+                   help="time the device-resident steps only (no e2e, output, forms, CPU): for profiling")
     return p.parse_args()
 
 
@@ -702,6 +704,15 @@ def run_ours(args):
     output = write_output(w, pos, u1d, stream) if (rank == 0 and not args.no_output) else None
     del u1d
 
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": "atoms/s", "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per_launch,
+                              "config": arm_config(args, w, args.precision, st["n_segments"], st["n_loopons"]),
+                              "note": "--kernel-only: device-resident steps alone"}), flush=True)
+        plan.close()
+        return
+
     # e2e: the public host call on pinned host memory
     e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
     hp = torch.empty((6, n), dtype=torch.float64, pin_memory=True)
@@ -722,6 +733,43 @@ def run_ours(args):
     e2e_t = max_over_ranks(e2e_t, world)
     e2e = {"value": n * world * e2e_steps / e2e_t, "unit": "atoms/s",
            "h2d_bytes_per_step": 6 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n, "steps": e2e_steps}
+    del hp, hv, atoms
+    # the same from the device lattice: sites built on the GPU (generateLattice
+    # order, bit-identical), loop tables from the host loops, the field, the
+    # displacements read back; nothing but the tables crosses to the device
+    e2e_lat = None
+    if w.cells[0] > 0:
+        import ctypes
+        lib = C.cuda_lib()
+        from disco_b200 import geometry as G
+        dl = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        ul = torch.empty((3, n), dtype=torch.float64, device="cuda")
+        hu = torch.empty((3, n), dtype=torch.float64, pin_memory=True)
+
+        def lat_step():
+            C.check(lib.disco_b200_lattice(w.lattice, w.cells[0], w.cells[1], w.cells[2], w.a0,
+                                           dl[0].data_ptr(), dl[1].data_ptr(), dl[2].data_ptr(),
+                                           ctypes.c_void_p(stream.cuda_stream)), lib)
+            ul.zero_()
+            pl = B.Plan(w.loops, w.box, precision=prec, images=w.images, nu=w.nu, max_atoms=n)
+            pl.execute(dl, ul)
+            hu.copy_(ul, non_blocking=True)
+            pl.sync(stream.cuda_stream)
+            pl.close()
+        lat_step()
+        same = bool(torch.equal(dl, pos))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            lat_step()
+        barrier()
+        tl = max_over_ranks(time.perf_counter() - t0, world)
+        e2e_lat = {"value": n * world * e2e_steps / tl, "unit": "atoms/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 3 * 8 * n, "steps": e2e_steps,
+                   "device_lattice_equals_host_lattice": same,
+                   "what": "disco_b200_lattice + plan (tables from the host loops) + field + displacements "
+                           "to pinned host memory, per step"}
+        del dl, ul, hu
 
     if rank == 0:
         fp64 = prec == C.DISCO_FP64
@@ -767,7 +815,7 @@ def run_ours(args):
             "dtype": "f64" if prec == C.DISCO_FP64 else "f32c", "data": "synthetic",
             "config": arm_config(args, w, args.precision, st["n_segments"], st["n_loopons"]),
             "evals_per_s": evals_atom * n * world * args.steps / elapsed,
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_device_lattice": e2e_lat, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps, "parity": parity, "output": output,
             **({"reference_gpu": refgpu} if refgpu else {}), **forms,
         }
@@ -1308,10 +1356,24 @@ def ctypes_byref(x):
     return ctypes.byref(x)
 
 
+def run_matter(args):
+    """--config matter: the matter step alone on the largest box the no-alloc
+    entry takes (compaction_rate), for profiling; one line."""
+    import torch
+    from disco_b200 import _capi as C
+    torch.cuda.set_device(dist_env()[2])
+    r = compaction_rate(C.cuda_lib(), C, torch, torch.cuda.current_stream())
+    print(json.dumps({"metric": "matter step atoms/s", "value": r["atoms_per_s"], "unit": "atoms/s",
+                      "config": {"workload": "bcc_prismatic 128^3 (4 194 304 atoms, 16 loops)"},
+                      "compaction": r}), flush=True)
+
+
 def main():
     args = parse()
     if args.precision is None:
         args.precision = "fp32c" if args.config == "batch" else "fp64"
+    if args.config == "matter":
+        return run_matter(args)
     if args.impl == "reference":
         run_reference(args)
     elif args.config == "batch":

@@ -190,9 +190,10 @@ class Plan:
     field into device arrays (torch tensors or raw device pointers)."""
 
     def __init__(self, loops, box, *, precision=C.DISCO_FP64, images=1, nu=0.35, image_split=0,
-                 max_atoms=0, image_min=0):
+                 max_atoms=0, image_min=0, near_plane=0.0, near_rim=0.0):
         self._lib = C.cuda_lib()
-        o = options(precision, images, nu, image_split, image_min=image_min)
+        o = options(precision, images, nu, image_split, image_min=image_min, near_plane=near_plane,
+                    near_rim=near_rim)
         arr, keep = loop_array(loops)
         b = (ctypes.c_double * 3)(*[float(v) for v in box])
         h = ctypes.c_void_p()
@@ -261,13 +262,14 @@ def sample_array(workloads, us=None, device_ptrs=None):
     return arr, keep
 
 
-def batch_gpu(workloads, precision=C.DISCO_FP64, nu=None, image_split=0, stage_kb=0, stages=0):
+def batch_gpu(workloads, precision=C.DISCO_FP64, nu=None, image_split=0, stage_kb=0, stages=0,
+              near_plane=0.0, near_rim=0.0):
     """The batched form on host arrays: returns [(ux, uy, uz)] per sample."""
     lib = C.cuda_lib()
     nu = workloads[0].nu if nu is None else nu
     us = [[np.zeros(w.n), np.zeros(w.n), np.zeros(w.n)] for w in workloads]
     arr, keep = sample_array(workloads, us)
-    o = options(precision, 1, nu, image_split)
+    o = options(precision, 1, nu, image_split, near_plane=near_plane, near_rim=near_rim)
     o.stage_kb = stage_kb
     o.stages = stages
     tm = C.DiscoTiming(0.0, 0.0, 0.0, None)

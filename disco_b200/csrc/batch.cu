@@ -55,6 +55,12 @@ struct BatchArgs {
     double cJ, cK, c2;
     float near_h, near_r;
     int* status;
+    // FP32 line form: (sample, atom) pairs with near-cut pairs, listed by the
+    // FP32 pass (near_mode 1); the unit-schedule FP64 pass (near_mode 2) runs
+    // only when the list overflowed (*near_count > near_cap)
+    int2* near_list;
+    unsigned int* near_count;
+    int32_t near_cap, near_mode;
 };
 
 constexpr int kBatchThreads = 256;
@@ -69,6 +75,7 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
     const int u0 = b.cta_first[blockIdx.x];
     const int nunits = b.cta_first[blockIdx.x + 1] - u0;
     if (nunits <= 0) return;
+    if (b.near_mode == 2 && *b.near_count <= (unsigned)b.near_cap) return;   // the listed pass ran
     const int D = b.stages;
     if (tid == 0) {
         for (int j = 0; j < D; ++j) mbar_init(&bar[j], 1);
@@ -119,6 +126,7 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
         fa.cJ = b.cJ; fa.cK = b.cK; fa.c2 = b.c2;
         fa.near_h = b.near_h; fa.near_r = b.near_r;
         fa.pieces64 = sd.pieces64; fa.segs64 = sd.segs64; fa.raw = sd.raw;
+        fa.near_list = nullptr; fa.near_count = nullptr; fa.near_cap = 0; fa.near_mode = 0;
         const unsigned char* st = stage0 + (size_t)buf * b.stage_bytes;
         Policy::template chunk<S>(fa, st, sd.chunks[un.chunk].npieces, split, px, py, pz, acc);
         if (un.last) {
@@ -135,11 +143,78 @@ __global__ void __launch_bounds__(kBatchThreads, Policy::kMinBlocks) batch_kerne
                 sd.uy[atom] += uy;
                 sd.uz[atom] += uz;
             }
+            if constexpr (Policy::kAppendsNear) {
+                if (b.near_mode == 1) {
+                    const int lane = tid & 31;
+                    const unsigned bn = __ballot_sync(0xffffffffu, acc.near);
+                    const unsigned grp = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane & ~(S - 1)));
+                    const bool app = valid && split == 0 && (bn & grp) != 0u;
+                    const unsigned ba = __ballot_sync(0xffffffffu, app);
+                    if (ba) {
+                        const int leader = __ffs(ba) - 1;
+                        unsigned q0 = 0;
+                        if (lane == leader) q0 = atomicAdd(b.near_count, (unsigned)__popc(ba));
+                        q0 = __shfl_sync(0xffffffffu, q0, leader);
+                        const unsigned q = q0 + (unsigned)__popc(ba & ((1u << lane) - 1u));
+                        if (app && q < (unsigned)b.near_cap) b.near_list[q] = make_int2(un.sample, (int)atom);
+                    }
+                }
+            }
         }
         __syncthreads();                           // every warp is done with stage[buf]
         if (tid == 0 && u + D < nunits) {
             fence_proxy_async_smem();
             issue(u + D);
+        }
+    }
+}
+
+// FP64 pass of the FP32 line form over the listed (sample, atom) pairs: S
+// lanes per pair split its images and walk the sample's chunks straight from
+// global memory (the few near atoms do not pay for staging); a fixed-order
+// butterfly sums the lanes, so each atom's result does not depend on the
+// list's order.  Returns at once when the list overflowed (the unit-schedule
+// pass runs instead).
+template <int S>
+__global__ void __launch_bounds__(kBatchThreads, 2) batch_near_list_kernel(const BatchArgs b)
+{
+    const unsigned cnt = *b.near_count;
+    if (cnt > (unsigned)b.near_cap) return;
+    const int tid = threadIdx.x;
+    const int split = tid % S;
+    constexpr int kPerCta = kBatchThreads / S;
+    FieldArgs fa;
+    fa.cJ = b.cJ; fa.cK = b.cK; fa.c2 = b.c2;
+    fa.near_h = b.near_h; fa.near_r = b.near_r;
+    fa.near_list = nullptr; fa.near_count = nullptr; fa.near_cap = 0; fa.near_mode = 0;
+    for (int64_t e0 = (int64_t)blockIdx.x * kPerCta; e0 < (int64_t)cnt; e0 += (int64_t)gridDim.x * kPerCta) {
+        const int64_t e = e0 + tid / S;
+        const bool valid = e < (int64_t)cnt;
+        const int2 pr = b.near_list[valid ? e : (int64_t)cnt - 1];
+        const SampleDev& sd = b.samples[pr.x];
+        const int64_t atom = pr.y;
+        fa.images = sd.images; fa.nimg = sd.nimg; fa.image_min = sd.image_min;
+        fa.Lx = sd.Lx; fa.Ly = sd.Ly; fa.Lz = sd.Lz;
+        fa.pieces64 = sd.pieces64; fa.segs64 = sd.segs64; fa.raw = sd.raw;
+        const double px = sd.x[atom], py = sd.y[atom], pz = sd.z[atom];
+        LineNearFp64::Acc acc;
+        acc.clear();
+        for (int c = 0; c < sd.nchunks; ++c) {
+            const Chunk ch = sd.chunks[c];
+            LineNearFp64::template chunk<S>(fa, sd.table + ch.offset, ch.npieces, split, px, py, pz, acc);
+        }
+        double ux, uy, uz;
+        acc.total(ux, uy, uz);
+#pragma unroll
+        for (int o = S / 2; o > 0; o >>= 1) {
+            ux += __shfl_xor_sync(0xffffffffu, ux, o);
+            uy += __shfl_xor_sync(0xffffffffu, uy, o);
+            uz += __shfl_xor_sync(0xffffffffu, uz, o);
+        }
+        if (valid && split == 0) {
+            sd.ux[atom] += ux;
+            sd.uy[atom] += uy;
+            sd.uz[atom] += uz;
         }
     }
 }
@@ -163,6 +238,10 @@ struct disco_batch_plan {
     int grid[2] = { 0, 0 };
     bool fp32 = false;
     int* d_status = nullptr;
+    int2* d_near = nullptr;                 // FP32 line form: (sample, atom) pairs with near-cut pairs
+    unsigned int* d_near_count = nullptr;
+    int32_t near_cap = 0;
+    int near_grid = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t captured_on = nullptr;
@@ -195,6 +274,8 @@ void free_batch(disco_batch_plan* p)
         if (p->d_cta_first[k]) cudaFree(p->d_cta_first[k]);
     }
     if (p->d_status) cudaFree(p->d_status);
+    if (p->d_near) cudaFree(p->d_near);
+    if (p->d_near_count) cudaFree(p->d_near_count);
     delete p;
 }
 
@@ -267,12 +348,29 @@ int launch_all(disco_batch_plan* p, cudaStream_t s)
         a.near_h = p->opt.near_plane > 0.0 ? (float)p->opt.near_plane : kNearPlane;
         a.near_r = p->opt.near_rim > 0.0 ? (float)p->opt.near_rim : kNearRim;
         a.status = p->d_status;
+        a.near_list = p->d_near;
+        a.near_count = p->d_near_count;
+        a.near_cap = p->near_cap;
         std::string err;
         int st;
         if (k == 0) {
-            st = p->fp32 ? launch_batch_policy<LineFp32>(a, p->grid[k], p->split, s, err)
-                         : launch_batch_policy<LineFp64>(a, p->grid[k], p->split, s, err);
-            if (!st && p->fp32) st = launch_batch_policy<LineNearFp64>(a, p->grid[k], p->split, s, err);
+            if (p->fp32) {
+                // FP32 pass listing the near atoms, the listed FP64 pass, and the
+                // unit-schedule FP64 pass that runs only if the list overflowed
+                cudaError_t e = cudaMemsetAsync(p->d_near_count, 0, sizeof(unsigned int), s);
+                if (e != cudaSuccess) return bfail(DISCO_ECUDA, cudaGetErrorString(e));
+                a.near_mode = 1;
+                st = launch_batch_policy<LineFp32>(a, p->grid[k], p->split, s, err);
+                if (!st) {
+                    batch_near_list_kernel<8><<<p->near_grid, kBatchThreads, 0, s>>>(a);
+                    e = cudaGetLastError();
+                    if (e != cudaSuccess) { err = cudaGetErrorString(e); st = DISCO_ECUDA; }
+                }
+                a.near_mode = 2;
+                if (!st) st = launch_batch_policy<LineNearFp64>(a, p->grid[k], p->split, s, err);
+            } else {
+                st = launch_batch_policy<LineFp64>(a, p->grid[k], p->split, s, err);
+            }
         } else {
             st = p->fp32 ? launch_batch_policy<LooponFp32>(a, p->grid[k], p->split, s, err)
                          : launch_batch_policy<LooponFp64>(a, p->grid[k], p->split, s, err);
@@ -465,6 +563,17 @@ int disco_b200_batch_plan_create(const disco_sample* samples, int32_t nsamples, 
         if (e != cudaSuccess) { free_batch(p); return bcuda(e, "batch queue upload"); }
         p->grid[k] = items.empty() ? 0 : grid;
         if (k == 0) p->stats.n_line_loops = 1; else p->stats.n_loopon_loops = 1;
+    }
+    if (p->fp32 && p->grid[0]) {
+        int64_t total = 0;
+        for (int s = 0; s < nsamples; ++s) total += samples[s].atoms.n;
+        p->near_cap = (int32_t)std::min<int64_t>(std::max<int64_t>(total, 1), 1 << 21);
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_near_list_kernel<8>, kBatchThreads, 0);
+        p->near_grid = std::max(1, p->sm_count * std::max(per_sm, 1));
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_near, (size_t)p->near_cap * sizeof(int2));
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_near_count, sizeof(unsigned int));
+        if (e != cudaSuccess) { free_batch(p); return bcuda(e, "near-cut list"); }
     }
     p->stage_bytes = (max_stage + 15) & ~15u;
     p->stats.n_loops = nsamples;

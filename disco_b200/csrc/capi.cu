@@ -2,6 +2,7 @@
 // device queries, plans (tables built and uploaded once), the resident
 // execute and the host-buffer drop-in that replaces kroupaGPU
 // (Code/backend_cuda.cu:568-722).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -31,6 +32,9 @@ struct disco_plan {
     unsigned char* d_table[2] = { nullptr, nullptr };
     disco::Chunk* d_chunks[2] = { nullptr, nullptr };
     int* d_status = nullptr;
+    int32_t* d_near = nullptr;               // FP32 line form: atoms with near-cut pairs
+    unsigned int* d_near_count = nullptr;
+    int32_t near_cap = 0;
     std::vector<double> loop_evals;          // per input loop: segments or loopons
     disco_plan_stats stats;
 };
@@ -89,6 +93,8 @@ void free_plan(disco_plan* p)
         if (p->d_chunks[k]) cudaFree(p->d_chunks[k]);
     }
     if (p->d_status) cudaFree(p->d_status);
+    if (p->d_near) cudaFree(p->d_near);
+    if (p->d_near_count) cudaFree(p->d_near_count);
     delete p;
 }
 
@@ -218,6 +224,14 @@ int disco_b200_plan_create(const disco_loop* loops, int32_t nloops, const double
     e = cudaMalloc(&p->d_status, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(p->d_status, 0, sizeof(int));
     if (e != cudaSuccess) { free_plan(p); return cuda_fail(e, "status word"); }
+    if (o.precision == DISCO_FP32C && !p->tables[0].chunks.empty()) {
+        // the list of atoms with near-cut pairs: up to 2^21 (a longer list
+        // overflows and the FP64 pass visits every atom)
+        p->near_cap = (int32_t)std::min<int64_t>(std::max<int64_t>(max_atoms, 1 << 16), 1 << 21);
+        e = cudaMalloc(&p->d_near, (size_t)p->near_cap * sizeof(int32_t));
+        if (e == cudaSuccess) e = cudaMalloc(&p->d_near_count, sizeof(unsigned int));
+        if (e != cudaSuccess) { free_plan(p); return cuda_fail(e, "near-cut list"); }
+    }
     *out = p;
     return DISCO_OK;
 }
@@ -259,6 +273,9 @@ int disco_b200_plan_execute(disco_plan* p, const disco_atoms* a, void* stream)
         if (T.fp32 && k == 0 && T.aux_pieces) {
             fa.pieces64 = reinterpret_cast<const disco::LinePiece*>(p->d_table[k] + T.aux_pieces);
             fa.segs64 = reinterpret_cast<const disco::LineSeg*>(p->d_table[k] + T.aux_segs);
+            fa.near_list = p->d_near;
+            fa.near_count = p->d_near_count;
+            fa.near_cap = p->near_cap;
         }
         std::string err;
         const int kind = k == 0 ? disco::kLineKind : disco::kLooponKind;

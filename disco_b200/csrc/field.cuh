@@ -133,6 +133,13 @@ struct FieldArgs {
     // line method: the loops' input vertices (x, y, z triplets), read only for
     // an atom on or within hband of a loop's plane
     const double* raw;
+    // FP32 line form: the atoms with at least one near-cut (piece, image).
+    // near_mode 1: the FP32 pass appends them (warp-aggregated, *near_count
+    // counts past near_cap); 2: the FP64 pass visits only the listed atoms, or
+    // every atom when the list overflowed; 0: no list (every atom).
+    int32_t* near_list;
+    unsigned int* near_count;
+    int32_t near_cap, near_mode;
 };
 
 // Host-side table: bytes + chunk list, built once per plan.

@@ -292,6 +292,7 @@ struct AccF64 {
 struct LineFp64 {
     using Acc = AccF64;
     static constexpr int kMinBlocks = 2;
+    static constexpr bool kAppendsNear = false;
     template <int S>
     static __device__ __forceinline__ void chunk(const FieldArgs& a, const unsigned char* st, int npieces,
                                                  int split, double px, double py, double pz, Acc& acc)
@@ -324,6 +325,7 @@ struct LineFp64 {
 struct LooponFp64 {
     using Acc = AccF64;
     static constexpr int kMinBlocks = 2;
+    static constexpr bool kAppendsNear = false;
     template <int S>
     static __device__ __forceinline__ void chunk(const FieldArgs& a, const unsigned char* st, int npieces,
                                                  int split, double px, double py, double pz, Acc& acc)
@@ -353,7 +355,14 @@ __global__ void __launch_bounds__(kThreads, Policy::kMinBlocks) field_kernel(con
     unsigned char* const stage0 = smem + kSmemHeader;
     const int tid = threadIdx.x;
     constexpr int kAtomsPerCta = kThreads / S;
-    const int64_t ntiles = (a.n + kAtomsPerCta - 1) / kAtomsPerCta;
+    // the atoms: all of them, or (FP64 near pass) those the FP32 pass listed
+    int64_t n = a.n;
+    const int32_t* list = nullptr;
+    if (a.near_mode == 2 && a.near_list) {
+        const unsigned c = *a.near_count;
+        if (c <= (unsigned)a.near_cap) { n = c; list = a.near_list; }
+    }
+    const int64_t ntiles = (n + kAtomsPerCta - 1) / kAtomsPerCta;
     if ((int64_t)blockIdx.x >= ntiles) return;
     const int nch = a.nchunks;
     const bool resident = a.resident != 0;
@@ -388,10 +397,11 @@ __global__ void __launch_bounds__(kThreads, Policy::kMinBlocks) field_kernel(con
         const int buf = resident ? 0 : (int)(u & 1);
         if (ch == 0) {
             const int64_t tile = (int64_t)blockIdx.x + tk * gridDim.x;
-            atom = tile * kAtomsPerCta + tid / S;
-            valid = atom < a.n;
-            const int64_t ia = valid ? atom : a.n - 1;
-            px = a.x[ia]; py = a.y[ia]; pz = a.z[ia];
+            const int64_t k = tile * kAtomsPerCta + tid / S;
+            valid = k < n;
+            const int64_t ik = valid ? k : n - 1;
+            atom = list ? (int64_t)list[ik] : ik;
+            px = a.x[atom]; py = a.y[atom]; pz = a.z[atom];
             acc.clear();
         }
         if (!resident || u == 0) {
@@ -424,6 +434,24 @@ __global__ void __launch_bounds__(kThreads, Policy::kMinBlocks) field_kernel(con
                 a.ux[atom] += ux;
                 a.uy[atom] += uy;
                 a.uz[atom] += uz;
+            }
+            if constexpr (Policy::kAppendsNear) {
+                if (a.near_mode == 1) {
+                    // list the atom if any of its S lanes met a near-cut pair
+                    const int lane = tid & 31;
+                    const unsigned b = __ballot_sync(0xffffffffu, acc.near);
+                    const unsigned grp = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane & ~(S - 1)));
+                    const bool app = valid && split == 0 && (b & grp) != 0u;
+                    const unsigned ba = __ballot_sync(0xffffffffu, app);
+                    if (ba) {
+                        const int leader = __ffs(ba) - 1;
+                        unsigned q0 = 0;
+                        if (lane == leader) q0 = atomicAdd(a.near_count, (unsigned)__popc(ba));
+                        q0 = __shfl_sync(0xffffffffu, q0, leader);
+                        const unsigned q = q0 + (unsigned)__popc(ba & ((1u << lane) - 1u));
+                        if (app && q < (unsigned)a.near_cap) a.near_list[q] = (int32_t)atom;
+                    }
+                }
             }
         }
         if (!resident) {

@@ -204,9 +204,24 @@ int launch_field_fp32(const FieldArgs& a0, int kind, int sm_count, int split_hin
     const size_t smem = kSmemHeader + (size_t)a.stage_bytes * (a.resident ? 1 : 2);
     const int S = split_hint > 0 ? split_hint : choose_split(a.n, a.nimg, sm_count * 2);
     if (kind != kLineKind) return launch_kind_f<LooponFp32>(a, S, sm_count, smem, stream, err);
+    if (!a.near_list) {
+        a.near_mode = 0;
+        const int st = launch_kind_f<LineFp32>(a, S, sm_count, smem, stream, err);
+        if (st) return st;
+        return launch_kind_f<LineNearFp64>(a, S, sm_count, smem, stream, err);
+    }
+    // the FP32 pass lists the atoms with near-cut pairs; the FP64 pass visits
+    // only those (every atom if the list overflowed), with its images split
+    // over 8 lanes since they are few
+    const cudaError_t e = cudaMemsetAsync(a.near_count, 0, sizeof(unsigned int), stream);
+    if (e != cudaSuccess) { err = cudaGetErrorString(e); return DISCO_ECUDA; }
+    a.near_mode = 1;
     const int st = launch_kind_f<LineFp32>(a, S, sm_count, smem, stream, err);
     if (st) return st;
-    return launch_kind_f<LineNearFp64>(a, S, sm_count, smem, stream, err);
+    a.near_mode = 2;
+    int Sn = 1;
+    while (Sn < 8 && 2 * Sn <= a.nimg) Sn *= 2;
+    return launch_kind_f<LineNearFp64>(a, split_hint > 0 ? S : Sn, sm_count, smem, stream, err);
 }
 
 } // namespace disco

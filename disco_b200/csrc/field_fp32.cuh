@@ -14,10 +14,12 @@ constexpr float kNearRim = 3.0f;     // A beyond the largest vertex radius
 struct AccF32K {
     float sx, sy, sz, cx, cy, cz;
     double dx, dy, dz;
+    bool near;                 // a near-cut pair was skipped (left to the FP64 pass)
     __device__ void clear()
     {
         sx = sy = sz = cx = cy = cz = 0.0f;
         dx = dy = dz = 0.0;
+        near = false;
     }
     __device__ __forceinline__ static void kahan(float& s, float& c, float v)
     {
@@ -177,6 +179,7 @@ __device__ __forceinline__ bool near_cut(const LinePieceF& pc, float Px, float P
 struct LineFp32 {
     using Acc = AccF32K;
     static constexpr int kMinBlocks = 2;
+    static constexpr bool kAppendsNear = true;
     template <int S>
     static __device__ __forceinline__ void chunk(const FieldArgs& a, const unsigned char* st, int npieces,
                                                  int split, double px, double py, double pz, Acc& acc)
@@ -191,7 +194,7 @@ struct LineFp32 {
                 double sx, sy, sz;
                 if (!image_shift(img, a.images, a.image_min, a.Lx, a.Ly, a.Lz, sx, sy, sz)) continue;
                 const float Px = (float)(qx - sx), Py = (float)(qy - sy), Pz = (float)(qz - sz);
-                if (near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) continue;
+                if (near_cut(pc, Px, Py, Pz, a.near_h, a.near_r)) { acc.near = true; continue; }
                 float fx = 0.0f, fy = 0.0f, fz = 0.0f;
                 line_piece_fp32(pc, recs + pc.rec, Px, Py, Pz, cJK2, fx, fy, fz);
                 acc.add(fx, fy, fz);
@@ -204,6 +207,7 @@ struct LineFp32 {
 struct LineNearFp64 {
     using Acc = AccF64;
     static constexpr int kMinBlocks = 2;
+    static constexpr bool kAppendsNear = false;
     template <int S>
     static __device__ __forceinline__ void chunk(const FieldArgs& a, const unsigned char* st, int npieces,
                                                  int split, double px, double py, double pz, Acc& acc)
@@ -244,6 +248,7 @@ struct LineNearFp64 {
 struct LooponFp32 {
     using Acc = AccF32K;
     static constexpr int kMinBlocks = 2;
+    static constexpr bool kAppendsNear = false;
     template <int S>
     static __device__ __forceinline__ void chunk(const FieldArgs& a, const unsigned char* st, int npieces,
                                                  int split, double px, double py, double pz, Acc& acc)

@@ -400,7 +400,10 @@ typedef struct {
  * (capacity copy_capacity) with their source renumbered and copies of removed
  * atoms dropped.  counts = {survivors, slab entries, copies}; when a capacity
  * is too small the call returns DISCO_ELIMIT with counts holding the sizes
- * needed.  Selection is bit-exact with the reference's FP64 predicate. */
+ * needed.  Selection is bit-exact with the reference's FP64 predicate.  On the
+ * device: one pass over the atoms (each atom's slab mask computed once,
+ * survivors compacted in order by decoupled look-back) and a short pass
+ * writing the slab entries and copies from the slab atoms' records. */
 int disco_b200_prismatic(const double *x, const double *y, const double *z, int64_t n,
                          const disco_slab_loop *loops, int32_t nloops, const double box[3],
                          double *x_out, double *y_out, double *z_out, int32_t *new_index,
@@ -415,18 +418,19 @@ int disco_b200_prismatic(const double *x, const double *y, const double *z, int6
  * No counterpart in the reference.  Inputs x, y, z and every output array
  * except info and counts are DEVICE pointers the caller allocated; loops,
  * box, info and counts are host memory.  Work is queued on `stream` (a
- * cudaStream_t; NULL = legacy default stream) and the call waits for it twice
- * to read the totals.  Scratch lives in a fixed 1.25 MiB device array inside
- * the library (held by every GPU that loads it until the process exits):
- * at most 4 194 304 atoms and 64 prismatic loops per call, DISCO_ELIMIT
- * beyond.  The first call on a device looks up that array's device address
- * (once per device), so make it before any stream capture.  All calls share
- * the array: calls whose work overlaps on the GPU (other streams, other host
+ * cudaStream_t; NULL = legacy default stream) and the call waits for it once,
+ * at the end, to read the totals.  Scratch lives in a fixed 3.25 MiB device
+ * array inside the library (held by every GPU that loads it until the process
+ * exits): at most 4 194 304 atoms, 64 prismatic loops and 65 536 atoms in
+ * slabs per call, DISCO_ELIMIT beyond.  The first call on a device looks up
+ * that array's device address (again after a device reset gives the device a
+ * new context), so make it before any stream capture.  All calls share the
+ * array: calls whose work overlaps on the GPU (other streams, other host
  * threads on the same device) race and must be serialised by the caller.
- * Capacities: slab_capacity as for disco_b200_prismatic; copies beyond
- * copy_capacity are not written and the call returns DISCO_ELIMIT with
- * counts[2] = copies needed.  The device outputs match disco_b200_prismatic's
- * bit for bit. */
+ * Capacities: slab entries beyond slab_capacity and copies beyond
+ * copy_capacity are not written, and the call returns DISCO_ELIMIT with
+ * counts[1] and counts[2] holding the sizes needed.  The device outputs match
+ * disco_b200_prismatic's bit for bit. */
 int disco_b200_prismatic_noalloc(const double *x, const double *y, const double *z, int64_t n,
                                  const disco_slab_loop *loops, int32_t nloops, const double box[3],
                                  double *x_out, double *y_out, double *z_out, int32_t *new_index,

@@ -90,3 +90,17 @@ def test_batch_rejects_bad_depth():
         B.batch_gpu(batch, C.DISCO_FP64, stages=5)
     with pytest.raises(C.DiscoError):
         B.batch_gpu(batch, C.DISCO_FP64, stage_kb=100, stages=3)
+
+
+def test_batch_near_list_and_its_overflow():
+    """FP32C batches with every pair near the cut: the FP64 pass over the
+    listed (sample, atom) pairs, and, beyond the list's 2^21 entries, the
+    unit-schedule FP64 pass, both reproduce the FP64 batch."""
+    small = _small_batch(seed=14, n=4)
+    big = W.batch(nsamples=3, edge=(80, 80), nloops=(1, 1), radius=(6.0, 8.0), segments=(16, 16),
+                  images=(1, 1), seed=15)                                # 3 x 1 024 000 atoms > 2^21
+    for batch in (small, big):
+        u64, _ = B.batch_gpu(batch, C.DISCO_FP64)
+        u32, _ = B.batch_gpu(batch, C.DISCO_FP32C, near_plane=1e6, near_rim=1e6)
+        for a, b in zip(u64, u32):
+            assert max(np.abs(a[k] - b[k]).max() for k in range(3)) <= 1e-12

@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 
 import oracle as O
+from disco_b200 import _capi as C
 from disco_b200 import backend as B
 from disco_b200 import workloads as W
 from disco_b200.backend import AtomArrays, GpuOptions
@@ -60,3 +61,28 @@ def test_fp32c_full_size_subsample(name):
     g = _run(w)
     ref = _oracle(w, atoms=(w.x[idx], w.y[idx], w.z[idx]))
     assert np.abs(g[idx] - ref).max() <= 2e-5
+
+
+def test_near_list_and_its_overflow():
+    """The FP32 pass lists the atoms with near-cut pairs and the FP64 pass
+    visits only those; the list holds max(max_atoms, 65536) atoms at most and a
+    longer one falls back to visiting every atom.  With every pair near, both
+    the listed and the overflowed plan reproduce the FP64 kernel."""
+    torch = pytest.importorskip("torch")
+    w = W.quadrupole(cells=40, radius=9.0, eps=0.0365)                 # 128 000 atoms
+    pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
+
+    def run(**kw):
+        p = B.Plan(w.loops, w.box, images=w.images, nu=w.nu, **kw)
+        u = torch.zeros_like(pos)
+        p.execute(pos, u)
+        p.sync(torch.cuda.current_stream().cuda_stream)
+        p.close()
+        return u.cpu().numpy()
+    f64 = run()
+    listed = run(precision=C.DISCO_FP32C, max_atoms=w.n, near_plane=1e6, near_rim=1e6)
+    overflow = run(precision=C.DISCO_FP32C, max_atoms=1, near_plane=1e6, near_rim=1e6)
+    assert np.abs(listed - f64).max() <= 1e-12
+    assert np.abs(overflow - f64).max() <= 1e-12
+    default = run(precision=C.DISCO_FP32C, max_atoms=w.n)
+    assert np.abs(default - f64).max() <= 2e-5

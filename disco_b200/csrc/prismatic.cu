@@ -136,6 +136,7 @@ constexpr int kMatterAtoms = 8;                                // per thread
 constexpr int kMatterTile = kMatterThreads * kMatterAtoms;     // 4096 atoms per tile
 constexpr int kMatterWarps = kMatterThreads / 32;
 constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // look-back categories
+constexpr size_t kMatterSmem = 2 * kMatterTile * sizeof(uint64_t); // masks and sides of a tile
 
 // Look-back words: flag in the top two bits, value below.
 constexpr unsigned long long kFlagAgg = 1ull << 62;
@@ -250,26 +251,31 @@ __device__ __forceinline__ void atom_masks(const SlabHead* sh, const SlabLoopDev
 
 // The matter step's single pass over the atoms.  Each CTA takes the next tile
 // of 4096 atoms (a ticket, so that every tile it looks back on belongs to a
-// CTA already running), reads its atoms once, computes every atom's slab mask
-// once (loops whose slab cannot reach the tile's bounding box are skipped for
-// the whole tile), counts per category, obtains its exclusive prefixes by
-// decoupled look-back over the preceding tiles' published counts, and writes
-// the survivors (x, y, z, new index) and the slab members' records at their
-// final ranks.  Bounded waits: a look-back that finds no count for 2 s
-// records DISCO_ETIMEOUT and publishes anyway, so no tile waits forever.
-__global__ void __launch_bounds__(kMatterThreads, 1) matter_pass_kernel(const MatterArgs a)
+// CTA already running); each warp owns 256 consecutive atoms of it (8 rounds
+// of 32, coalesced), reads them once, takes their bounding box and skips every
+// loop whose slab cannot reach it, and computes each atom's slab mask once
+// (kept in shared memory for the ranked writes).  Per category the tile's
+// count is published and its exclusive prefix obtained by decoupled
+// look-back over the preceding tiles' published counts; survivors (x, y, z,
+// new index) and the slab members' records are then written at their final
+// ranks.  Bounded waits: a look-back that finds no count for 2 s records
+// DISCO_ETIMEOUT and publishes anyway, so no tile waits forever.
+// Dynamic shared memory: kMatterTile masks and sides (64 KB).
+__global__ void __launch_bounds__(kMatterThreads, 2) matter_pass_kernel(const MatterArgs a)
 {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    uint64_t* smask = reinterpret_cast<uint64_t*>(dyn);
+    uint64_t* ssides = smask + kMatterTile;
     __shared__ SlabHead sh[kMaxSlabLoops];
-    __shared__ double red[6][kMatterWarps];
-    __shared__ unsigned long long tmask_s;
-    __shared__ int cnt_s[kMatterAtoms * kMatterWarps];         // survivors per (round, warp), then prefixes
-    __shared__ int cnt_m[kMatterAtoms * kMatterWarps];         // members per (round, warp), then prefixes
+    __shared__ int cnt_s[kMatterWarps * kMatterAtoms];         // survivors per (warp, round), then prefixes
+    __shared__ int cnt_m[kMatterWarps * kMatterAtoms];         // members per (warp, round), then prefixes
     __shared__ int cnt_c[2 * kMaxSlabLoops];                   // slab and kept-copy counts per loop
     __shared__ int64_t excl[kMaxCats];
+    __shared__ unsigned long long vac_s;
     __shared__ int tile_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nl = a.nl, C = a.C;
-    if (tid == 0) { tile_s = (int)atomicAdd(a.ticket, 1u); tmask_s = 0ull; }
+    if (tid == 0) { tile_s = (int)atomicAdd(a.ticket, 1u); vac_s = 0ull; }
     {
         const int words = nl * (int)(sizeof(SlabHead) / 8);
         const uint64_t* src = reinterpret_cast<const uint64_t*>(a.heads);
@@ -278,15 +284,16 @@ __global__ void __launch_bounds__(kMatterThreads, 1) matter_pass_kernel(const Ma
         for (int i = tid; i < 2 * nl; i += kMatterThreads) cnt_c[i] = 0;
     }
     __syncthreads();
+    if (tid < nl && sh[tid].type == DISCO_MATTER_VACANCY) atomicOr(&vac_s, 1ull << tid);
     const int64_t tile = tile_s;
-    const int64_t base = tile * kMatterTile;
+    const int64_t wbase = tile * kMatterTile + (int64_t)warp * (32 * kMatterAtoms);   // this warp's atoms
 
-    // the tile's bounding box (the atoms are read from HBM here; the two later
-    // passes over the same 96 KB find them in L1/L2)
+    // the warp's bounding box (its atoms come from HBM here; the later reads
+    // of the same 6 KB hit L1/L2) and the loops whose slab can reach it
     double lo[3] = { 1e300, 1e300, 1e300 }, hi[3] = { -1e300, -1e300, -1e300 };
 #pragma unroll
     for (int r = 0; r < kMatterAtoms; ++r) {
-        const int64_t i = base + r * kMatterThreads + tid;
+        const int64_t i = wbase + r * 32 + lane;
         if (i < a.n) {
             const double px = a.x[i], py = a.y[i], pz = a.z[i];
             lo[0] = fmin(lo[0], px); hi[0] = fmax(hi[0], px);
@@ -294,6 +301,7 @@ __global__ void __launch_bounds__(kMatterThreads, 1) matter_pass_kernel(const Ma
             lo[2] = fmin(lo[2], pz); hi[2] = fmax(hi[2], pz);
         }
     }
+    uint64_t wmask = 0;
     if (nl > 0) {
 #pragma unroll
         for (int k = 0; k < 3; ++k)
@@ -301,45 +309,37 @@ __global__ void __launch_bounds__(kMatterThreads, 1) matter_pass_kernel(const Ma
                 lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
                 hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
             }
-        if (lane == 0)
-            for (int k = 0; k < 3; ++k) { red[k][warp] = lo[k]; red[3 + k][warp] = hi[k]; }
-        __syncthreads();
-        if (tid < nl) {
-            double b[6];
-            for (int k = 0; k < 3; ++k) {
-                b[k] = red[k][0]; b[3 + k] = red[3 + k][0];
-                for (int w = 1; w < kMatterWarps; ++w) {
-                    b[k] = fmin(b[k], red[k][w]);
-                    b[3 + k] = fmax(b[3 + k], red[3 + k][w]);
-                }
+        for (int half = 0; half < 2; ++half) {
+            const int l = lane + 32 * half;
+            bool reach = false;
+            if (l < nl && lo[0] <= hi[0]) {
+                const SlabHead& S = sh[l];
+                const double gx = periodic_gap(lo[0], hi[0], S.cx, a.Lx);
+                const double gy = periodic_gap(lo[1], hi[1], S.cy, a.Ly);
+                const double gz = periodic_gap(lo[2], hi[2], S.cz, a.Lz);
+                reach = !(gx * gx + gy * gy + gz * gz > S.bound * S.bound);
             }
-            const SlabHead& S = sh[tid];
-            const double gx = periodic_gap(b[0], b[3], S.cx, a.Lx);
-            const double gy = periodic_gap(b[1], b[4], S.cy, a.Ly);
-            const double gz = periodic_gap(b[2], b[5], S.cz, a.Lz);
-            if (!(gx * gx + gy * gy + gz * gz > S.bound * S.bound)) atomicOr(&tmask_s, 1ull << tid);
+            wmask |= (uint64_t)__ballot_sync(0xffffffffu, reach) << (32 * half);
         }
-        __syncthreads();
     }
-    const uint64_t tmask = tmask_s;
+    __syncthreads();                                        // vac_s
+    const uint64_t vac = vac_s;
 
-    // every atom's mask, once
-    uint64_t mask[kMatterAtoms], sides[kMatterAtoms];
-    unsigned rem = 0, val = 0;
-#pragma unroll
+    // every atom's mask, once; counts per (warp, round) and per loop
+    const int wt = warp * (32 * kMatterAtoms);              // the warp's first atom in the tile
+#pragma unroll 1
     for (int r = 0; r < kMatterAtoms; ++r) {
-        const int64_t i = base + r * kMatterThreads + tid;
+        const int64_t i = wbase + r * 32 + lane;
+        const bool valid = i < a.n;
+        uint64_t mask = 0, sides = 0;
         bool removed = false;
-        mask[r] = 0; sides[r] = 0;
-        if (i < a.n) {
-            val |= 1u << r;
-            if (tmask) atom_masks(sh, a.loops, tmask, a.x[i], a.y[i], a.z[i], a, mask[r], sides[r], removed);
-        }
-        if (removed) rem |= 1u << r;
-        const unsigned bs = __ballot_sync(0xffffffffu, ((val >> r) & 1u) && !removed);
-        const unsigned bm = __ballot_sync(0xffffffffu, mask[r] != 0);
-        if (lane == 0) { cnt_s[r * kMatterWarps + warp] = __popc(bs); cnt_m[r * kMatterWarps + warp] = __popc(bm); }
-        for (uint64_t m = mask[r]; m; m &= m - 1) {            // members are rare
+        if (valid && wmask) atom_masks(sh, a.loops, wmask, a.x[i], a.y[i], a.z[i], a, mask, sides, removed);
+        smask[wt + r * 32 + lane] = mask;
+        ssides[wt + r * 32 + lane] = sides;
+        const unsigned bs = __ballot_sync(0xffffffffu, valid && !removed);
+        const unsigned bm = __ballot_sync(0xffffffffu, mask != 0);
+        if (lane == 0) { cnt_s[warp * kMatterAtoms + r] = __popc(bs); cnt_m[warp * kMatterAtoms + r] = __popc(bm); }
+        for (uint64_t m = mask; m; m &= m - 1) {             // members are rare
             const int l = __ffsll((long long)m) - 1;
             atomicAdd(&cnt_c[l], 1);
             if (sh[l].type == DISCO_MATTER_INTERSTITIAL && !removed) atomicAdd(&cnt_c[nl + l], 1);
@@ -347,29 +347,10 @@ __global__ void __launch_bounds__(kMatterThreads, 1) matter_pass_kernel(const Ma
     }
     __syncthreads();
 
-    // tile totals, then prefixes over (round, warp) in atom order
-    if (warp == 0 || warp == 1) {
-        int* cnt = warp == 0 ? cnt_s : cnt_m;
-        constexpr int kPer = kMatterAtoms * kMatterWarps / 32;  // 4 entries per lane
-        int v[kPer], tot = 0;
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) { v[j] = cnt[lane * kPer + j]; tot += v[j]; }
-        int incl = tot;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        int run = incl - tot;
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) { cnt[lane * kPer + j] = run; run += v[j]; }
-        if (lane == 31) excl[warp] = incl;                     // tile aggregate (temporarily)
-    }
-    __syncthreads();
-
-    // decoupled look-back, one thread per category
-    if (tid < C) {
-        const int c = tid;
-        const int64_t agg = c == 0 ? excl[0] : c == 1 ? excl[1] : (int64_t)cnt_c[c - 2];
+    // warps 0 and 1: prefixes over (warp, round) in atom order, the tile's
+    // survivor and member counts and their look-back; threads 64.. : the
+    // look-back of the per-loop categories
+    auto look_back = [&](int c, int64_t agg) {
         unsigned long long* my = a.status + tile * C + c;
         int64_t prefix = 0;
         if (tile == 0) {
@@ -395,35 +376,54 @@ __global__ void __launch_bounds__(kMatterThreads, 1) matter_pass_kernel(const Ma
         }
         a.tile_excl[tile * C + c] = (int32_t)prefix;
         excl[c] = prefix;
+    };
+    if (warp < 2) {
+        int* cnt = warp == 0 ? cnt_s : cnt_m;
+        constexpr int kPer = kMatterAtoms * kMatterWarps / 32;  // 4 entries per lane
+        int v[kPer], tot = 0;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) { v[j] = cnt[lane * kPer + j]; tot += v[j]; }
+        int incl = tot;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        int run = incl - tot;
+#pragma unroll
+        for (int j = 0; j < kPer; ++j) { cnt[lane * kPer + j] = run; run += v[j]; }
+        if (lane == 31) look_back(warp, incl);
+    } else if (tid - 64 < C - 2) {
+        look_back(tid - 62, (int64_t)cnt_c[tid - 64]);
     }
     __syncthreads();
 
     // survivors at their final ranks, the new-index map, member records
     const unsigned ltm = (1u << lane) - 1u;
-#pragma unroll
+#pragma unroll 2
     for (int r = 0; r < kMatterAtoms; ++r) {
-        const int64_t i = base + r * kMatterThreads + tid;
-        const bool valid = (val >> r) & 1u;
-        const bool surv = valid && !((rem >> r) & 1u);
+        const int64_t i = wbase + r * 32 + lane;
+        const bool valid = i < a.n;
+        const uint64_t mask = smask[wt + r * 32 + lane];
+        const bool surv = valid && !(mask & vac);
         const unsigned bs = __ballot_sync(0xffffffffu, surv);
-        const unsigned bm = __ballot_sync(0xffffffffu, mask[r] != 0);
+        const unsigned bm = __ballot_sync(0xffffffffu, mask != 0);
         if (valid) {
             if (surv) {
-                const int64_t q = excl[0] + cnt_s[r * kMatterWarps + warp] + __popc(bs & ltm);
+                const int64_t q = excl[0] + cnt_s[warp * kMatterAtoms + r] + __popc(bs & ltm);
                 if (q < a.n) { a.xo[q] = a.x[i]; a.yo[q] = a.y[i]; a.zo[q] = a.z[i]; }
                 a.new_index[i] = (int32_t)q;
             } else {
                 a.new_index[i] = -1;
             }
         }
-        if (mask[r]) {
-            const int64_t q = excl[1] + cnt_m[r * kMatterWarps + warp] + __popc(bm & ltm);
+        if (mask) {
+            const int64_t q = excl[1] + cnt_m[warp * kMatterAtoms + r] + __popc(bm & ltm);
             if (q < a.member_cap) {
                 MemberRec m;
                 m.atom = (int32_t)i;
-                m.removed = (rem >> r) & 1u;
-                m.mask = mask[r];
-                m.sides = sides[r];
+                m.removed = (mask & vac) != 0;
+                m.mask = mask;
+                m.sides = ssides[wt + r * 32 + lane];
                 a.members[q] = m;
             }
         }
@@ -679,21 +679,50 @@ unsigned char g_stage_bytes[sizeof(LoopStage)];
 
 size_t recs_offset(int nl) { return ((size_t)nl * sizeof(disco::SlabHead) + 15) & ~size_t(15); }
 
+// What the last upload into the no-alloc scratch held (device, context,
+// bytes): a call with the same loops on the same device skips the upload,
+// since every call waits for its own work before it returns.
+struct StageCache {
+    unsigned char* dst = nullptr;
+    unsigned long long ctx = 0;
+    size_t bytes = 0;
+    unsigned char data[sizeof(LoopStage)];
+};
+StageCache g_stage_cache;
+
+void stage_cache_drop()
+{
+    std::lock_guard<std::mutex> lock(g_stage_mutex);
+    g_stage_cache.dst = nullptr;
+}
+
 // prepare_loops into the staging buffer, then one upload of its used bytes
-// to dst on stream s.
+// to dst on stream s (skipped when `ctx` is non-zero and the same bytes were
+// the last ones uploaded to dst in that context).
 int stage_loops(const disco_slab_loop* loops, int nloops, const double box[3], disco_slab_info* info,
-                int* act_index, int& nl, unsigned char* dst, cudaStream_t s)
+                int* act_index, int& nl, unsigned char* dst, cudaStream_t s, unsigned long long ctx = 0)
 {
     std::lock_guard<std::mutex> lock(g_stage_mutex);
     int st = prepare_loops(loops, nloops, box, info, g_stage_parts.heads, g_stage_parts.recs, act_index, nl);
     if (st || nl == 0) return st;
     const size_t hb = (size_t)nl * sizeof(disco::SlabHead), off = recs_offset(nl);
+    const size_t bytes = off + (size_t)nl * sizeof(disco::SlabLoopDev);
     std::memcpy(g_stage_bytes, g_stage_parts.heads, hb);
     std::memset(g_stage_bytes + hb, 0, off - hb);
     std::memcpy(g_stage_bytes + off, g_stage_parts.recs, (size_t)nl * sizeof(disco::SlabLoopDev));
-    const cudaError_t e = cudaMemcpyAsync(dst, g_stage_bytes, off + (size_t)nl * sizeof(disco::SlabLoopDev),
-                                          cudaMemcpyHostToDevice, s);
-    return e == cudaSuccess ? DISCO_OK : cfail(e, "loop table upload");
+    if (ctx && g_stage_cache.dst == dst && g_stage_cache.ctx == ctx && g_stage_cache.bytes == bytes &&
+        std::memcmp(g_stage_cache.data, g_stage_bytes, bytes) == 0)
+        return DISCO_OK;
+    g_stage_cache.dst = nullptr;
+    const cudaError_t e = cudaMemcpyAsync(dst, g_stage_bytes, bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cfail(e, "loop table upload");
+    if (ctx) {
+        g_stage_cache.dst = dst;
+        g_stage_cache.ctx = ctx;
+        g_stage_cache.bytes = bytes;
+        std::memcpy(g_stage_cache.data, g_stage_bytes, bytes);
+    }
+    return DISCO_OK;
 }
 
 // Bytes of the look-back words (ticket and error word first).
@@ -727,8 +756,10 @@ int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int
     a.totals = m.totals;
     e = cudaMemsetAsync(m.status, 0, status_bytes(ntiles, a.C), s);
     if (e != cudaSuccess) return cfail(e, "look-back reset");
+    e = cudaFuncSetAttribute(matter_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMatterSmem);
+    if (e != cudaSuccess) return cfail(e, "matter step shared memory");
     if (ntiles > 0) {
-        matter_pass_kernel<<<(unsigned)ntiles, kMatterThreads, 0, s>>>(a);
+        matter_pass_kernel<<<(unsigned)ntiles, kMatterThreads, kMatterSmem, s>>>(a);
         matter_tail_kernel<<<(unsigned)ntiles, 256, 0, s>>>(a, ntiles);
     } else {
         e = cudaMemsetAsync(m.totals, 0, (size_t)(a.C + 1) * sizeof(int64_t), s);
@@ -1018,7 +1049,7 @@ unsigned long long current_context_id()
 // looked up with that device current and cached with the identifier of the
 // context it belongs to; a new context on that device (after a device reset,
 // which reloads the module) gets a fresh lookup.
-int noalloc_scratch(unsigned char** out)
+int noalloc_scratch(unsigned char** out, unsigned long long* ctx_out)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -1037,6 +1068,7 @@ int noalloc_scratch(unsigned char** out)
         g_noalloc_ctx[dev] = ctx;
     }
     *out = g_noalloc_addr[dev];
+    *ctx_out = ctx;
     return DISCO_OK;
 }
 
@@ -1065,12 +1097,13 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     if (cudaGetDeviceCount(&dcount) != cudaSuccess || dcount == 0) return efail(DISCO_ENODEV, "no CUDA device");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* base = nullptr;
-    int st = noalloc_scratch(&base);
+    unsigned long long ctx = 0;
+    int st = noalloc_scratch(&base, &ctx);
     if (st) return st;
 
     int act_index[kMaxSlabLoops];
     int nl = 0;
-    st = stage_loops(loops, nloops, box, info, act_index, nl, base + kNoAllocLoopOff, s);
+    st = stage_loops(loops, nloops, box, info, act_index, nl, base + kNoAllocLoopOff, s, ctx);
     if (st) return st;
     const int C = 2 + 2 * nl;
     const int64_t ntiles = (n + kMatterTile - 1) / kMatterTile;
@@ -1097,11 +1130,11 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     m.member_cap = member_cap;
     m.totals = reinterpret_cast<int64_t*>(base + kNoAllocTotalsOff);
     st = matter_queue(a, m, nl, ntiles, s);
-    if (st) return st;
+    if (st) { stage_cache_drop(); return st; }
     int64_t tot[kMaxCats + 1];
     cudaError_t e = cudaMemcpyAsync(tot, m.totals, (size_t)(C + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cfail(e, "prismatic totals");
+    if (e != cudaSuccess) { stage_cache_drop(); return cfail(e, "prismatic totals"); }
     st = matter_finish(tot, nl, act_index, nloops, info, slab_capacity, copy_capacity, member_cap, counts);
     if (st == DISCO_ELIMIT && tot[1] > member_cap && counts[1] <= slab_capacity && counts[2] <= copy_capacity)
         return efail(DISCO_ELIMIT, "disco_b200_prismatic_noalloc takes at most 65536 atoms in slabs "

@@ -925,13 +925,15 @@ def run_batch(args):
         e2e = {"value": n * world / e2e_t, "unit": "atoms/s", "h2d_bytes_per_step": 48 * n,
                "d2h_bytes_per_step": 24 * n, "steps": 1}
     if rank == 0:
-        peak = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else fp32_peak_tflops(torch)
+        gemm = fp64_peak_tflops(torch) if prec == C.DISCO_FP64 else fp32_peak_tflops(torch)
+        peak, peak_src = pipe_peak_tflops(torch, clk, prec == C.DISCO_FP64)
         achieved = evals * W_LINE / per / 1e12
         roof = {"bound": "fp32" if prec != C.DISCO_FP64 else "fp64", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "flop_per_eval": W_LINE,
-                "evals_per_launch": evals,
-                "peak_source": "measured here: torch " + ("DGEMM" if prec == C.DISCO_FP64 else
-                                                          "SGEMM without TF32") + " 8192^3, best of 5"}
+                "evals_per_launch": evals, "peak_source": peak_src, "peak_gemm": gemm,
+                "frac_of_gemm": achieved / gemm,
+                "peak_gemm_source": "measured here: torch " + ("DGEMM" if prec == C.DISCO_FP64 else
+                                                               "SGEMM without TF32") + " 8192^3, best of 5"}
         line = {
             "metric": METRIC, "value": n * world / per, "unit": "atoms/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * per,

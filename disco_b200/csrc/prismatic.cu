@@ -131,9 +131,9 @@ struct MemberRec {
     uint64_t mask, sides;
 };
 
-constexpr int kMatterThreads = 512;
+constexpr int kMatterThreads = 256;
 constexpr int kMatterAtoms = 8;                                // per thread
-constexpr int kMatterTile = kMatterThreads * kMatterAtoms;     // 4096 atoms per tile
+constexpr int kMatterTile = kMatterThreads * kMatterAtoms;     // 2048 atoms per tile
 constexpr int kMatterWarps = kMatterThreads / 32;
 constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // look-back categories
 constexpr size_t kMatterSmem = 2 * kMatterTile * sizeof(uint64_t); // masks and sides of a tile
@@ -250,7 +250,7 @@ __device__ __forceinline__ void atom_masks(const SlabHead* sh, const SlabLoopDev
 }
 
 // The matter step's single pass over the atoms.  Each CTA takes the next tile
-// of 4096 atoms (a ticket, so that every tile it looks back on belongs to a
+// of 2048 atoms (a ticket, so that every tile it looks back on belongs to a
 // CTA already running); each warp owns 256 consecutive atoms of it (8 rounds
 // of 32, coalesced), reads them once, takes their bounding box and skips every
 // loop whose slab cannot reach it, and computes each atom's slab mask once
@@ -260,8 +260,9 @@ __device__ __forceinline__ void atom_masks(const SlabHead* sh, const SlabLoopDev
 // new index) and the slab members' records are then written at their final
 // ranks.  Bounded waits: a look-back that finds no count for 2 s records
 // DISCO_ETIMEOUT and publishes anyway, so no tile waits forever.
-// Dynamic shared memory: kMatterTile masks and sides (64 KB).
-__global__ void __launch_bounds__(kMatterThreads, 2) matter_pass_kernel(const MatterArgs a)
+// Dynamic shared memory: kMatterTile masks and sides (32 KB); four CTAs per
+// SM, so that one CTA's barriers and look-back overlap the others' loads.
+__global__ void __launch_bounds__(kMatterThreads, 4) matter_pass_kernel(const MatterArgs a)
 {
     extern __shared__ __align__(16) unsigned char dyn[];
     uint64_t* smask = reinterpret_cast<uint64_t*>(dyn);
@@ -379,7 +380,7 @@ __global__ void __launch_bounds__(kMatterThreads, 2) matter_pass_kernel(const Ma
     };
     if (warp < 2) {
         int* cnt = warp == 0 ? cnt_s : cnt_m;
-        constexpr int kPer = kMatterAtoms * kMatterWarps / 32;  // 4 entries per lane
+        constexpr int kPer = kMatterAtoms * kMatterWarps / 32;  // 2 entries per lane
         int v[kPer], tot = 0;
 #pragma unroll
         for (int j = 0; j < kPer; ++j) { v[j] = cnt[lane * kPer + j]; tot += v[j]; }
@@ -392,8 +393,9 @@ __global__ void __launch_bounds__(kMatterThreads, 2) matter_pass_kernel(const Ma
 #pragma unroll
         for (int j = 0; j < kPer; ++j) { cnt[lane * kPer + j] = run; run += v[j]; }
         if (lane == 31) look_back(warp, incl);
-    } else if (tid - 64 < C - 2) {
-        look_back(tid - 62, (int64_t)cnt_c[tid - 64]);
+    } else {
+        for (int c = tid - 62; c < C; c += kMatterThreads - 64)     // up to 128 per-loop categories
+            look_back(c, (int64_t)cnt_c[c - 2]);
     }
     __syncthreads();
 
@@ -756,8 +758,10 @@ int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int
     a.totals = m.totals;
     e = cudaMemsetAsync(m.status, 0, status_bytes(ntiles, a.C), s);
     if (e != cudaSuccess) return cfail(e, "look-back reset");
-    e = cudaFuncSetAttribute(matter_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMatterSmem);
-    if (e != cudaSuccess) return cfail(e, "matter step shared memory");
+    if (kMatterSmem > 48 * 1024) {
+        e = cudaFuncSetAttribute(matter_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMatterSmem);
+        if (e != cudaSuccess) return cfail(e, "matter step shared memory");
+    }
     if (ntiles > 0) {
         matter_pass_kernel<<<(unsigned)ntiles, kMatterThreads, kMatterSmem, s>>>(a);
         matter_tail_kernel<<<(unsigned)ntiles, 256, 0, s>>>(a, ntiles);
@@ -988,7 +992,7 @@ int disco_b200_finalize_resident(const double* x, const double* y, const double*
 // does, a process with a fixed memory budget) cannot let the library call
 // cudaMalloc.  disco_b200_prismatic_noalloc takes device inputs and outputs
 // from the caller and keeps its scratch (loop table, look-back words, per-tile
-// prefixes, member records, totals) in the file-scope array below: 3.25 MiB
+// prefixes, member records, totals) in the file-scope array below: 5 MiB
 // that every GPU loading this library holds until the process exits.
 
 namespace {
@@ -1005,7 +1009,7 @@ constexpr size_t kNoAllocMemberOff =
     kNoAllocExclOff + align256c((size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(int32_t));
 constexpr size_t kNoAllocTotalsOff =
     kNoAllocMemberOff + align256c((size_t)kNoAllocMaxMembers * sizeof(disco::MemberRec));
-constexpr size_t kNoAllocScratchBytes = 3328 * 1024;
+constexpr size_t kNoAllocScratchBytes = 5 * 1024 * 1024;
 static_assert(kNoAllocTotalsOff + (disco::kMaxCats + 1) * sizeof(int64_t) <= kNoAllocScratchBytes,
               "no-alloc scratch layout");
 

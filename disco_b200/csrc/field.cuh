@@ -42,7 +42,7 @@ struct alignas(16) LineSeg {
     double tx, ty, tz;   // unit tangent (B - A) / |B - A| (0 for a null segment)
     double wx, wy, wz;   // w = b x t
     double nx, ny, nz;   // (A - apex) x (B - apex)
-    double pad;
+    double hl2;          // |B - A|^2 / 2
 };
 static_assert(sizeof(LinePiece) == 144 && sizeof(LineSeg) == 112, "line table layout");
 

@@ -116,7 +116,7 @@ __device__ __forceinline__ void line_segments(const LineSeg* seg, int nseg, doub
 
         // solid angle of triangle (apex, A, B), Code/barnett.hpp:69-72 times l1 la lb;
         // e.(a x b) = e.((A - apex) x (B - apex)) as e is along apex - P
-        const double den = fma(ea, lb, fma(eb, la, fma(la, lb, ax * bx + ay * by + az * bz)));
+        const double den = fma(ea, lb, fma(eb, la, fma(la, lb, fma(0.5, la2 + lb2, -s.hl2))));   // a.b = (|a|^2 + |b|^2 - L^2) / 2
         const double num = ex * s.nx + ey * s.ny + ez * s.nz;
         const double nzr = zr * den - zi * num;
         zi = zr * num + zi * den;
@@ -536,6 +536,7 @@ inline void make_line_piece(const disco_loop& lp, int k0, int k1e, double bx, do
             s.wy = cK * (bz * s.tx - bx * s.tz);
             s.wz = cK * (bx * s.ty - by * s.tx);
         }
+        s.hl2 = 0.5 * L * L;
         p.rho = std::max(p.rho, radius(k));
         p.lmax = std::max(p.lmax, L);
         recs.push_back(s);

@@ -138,10 +138,10 @@ constexpr int kMatterWarps = kMatterThreads / 32;
 constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // look-back categories
 constexpr size_t kMatterSmem = 2 * kMatterTile * sizeof(uint64_t); // masks and sides of a tile
 
-// Look-back words: flag in the top two bits, value below.
-constexpr unsigned long long kFlagAgg = 1ull << 62;
-constexpr unsigned long long kFlagInc = 2ull << 62;
-constexpr unsigned long long kValMask = (1ull << 62) - 1;
+// Tile flags of the look-back: 0 not yet published, 1 the tile's counts
+// (agg) are published, 2 its inclusive prefixes (inc) are too.
+constexpr int kFlagAgg = 1;
+constexpr int kFlagInc = 2;
 
 struct MatterArgs {
     const double *x, *y, *z;
@@ -153,9 +153,10 @@ struct MatterArgs {
     double Lx, Ly, Lz;
     float iLx, iLy, iLz;          // 1 / box lengths in FP32 (the pre-test only)
     int32_t pad_;
-    unsigned long long* status;   // [ntiles][C] look-back words, zeroed per call
+    int* flags;                   // [ntiles] look-back flags, zeroed per call
     unsigned int* ticket;         // tile counter, zeroed per call
-    int32_t* tile_excl;           // [ntiles][C] exclusive prefixes
+    int32_t* agg;                 // [ntiles][C] the tile's counts
+    int32_t* inc;                 // [ntiles][C] inclusive prefixes (exclusive = inc - agg)
     MemberRec* members;
     int64_t member_cap;
     double *xo, *yo, *zo;
@@ -169,15 +170,15 @@ struct MatterArgs {
     int* err;
 };
 
-__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v)
+__device__ __forceinline__ void st_release(int* p, int v)
 {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
 }
 
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p)
+__device__ __forceinline__ int ld_acquire(const int* p)
 {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
 
@@ -272,6 +273,8 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_pass_kernel(const Ma
     __shared__ int cnt_m[kMatterWarps * kMatterAtoms];         // members per (warp, round), then prefixes
     __shared__ int cnt_c[2 * kMaxSlabLoops];                   // slab and kept-copy counts per loop
     __shared__ int64_t excl[kMaxCats];
+    __shared__ int aggv[2];
+    __shared__ int s_k;
     __shared__ unsigned long long vac_s;
     __shared__ int tile_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -348,36 +351,8 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_pass_kernel(const Ma
     }
     __syncthreads();
 
-    // warps 0 and 1: prefixes over (warp, round) in atom order, the tile's
-    // survivor and member counts and their look-back; threads 64.. : the
-    // look-back of the per-loop categories
-    auto look_back = [&](int c, int64_t agg) {
-        unsigned long long* my = a.status + tile * C + c;
-        int64_t prefix = 0;
-        if (tile == 0) {
-            st_release(my, kFlagInc | (unsigned long long)agg);
-        } else {
-            st_release(my, kFlagAgg | (unsigned long long)agg);
-            int64_t j = tile - 1;
-            unsigned long long t0 = 0;
-            while (true) {
-                const unsigned long long v = ld_acquire(a.status + j * C + c);
-                const unsigned long long f = v & ~kValMask;
-                if (f == 0) {
-                    if (t0 == 0) t0 = global_ns();
-                    else if (global_ns() - t0 > kWaitLimitNs) { report(a.err, DISCO_ETIMEOUT); break; }
-                    continue;
-                }
-                prefix += (int64_t)(v & kValMask);
-                if (f == kFlagInc || j == 0) break;
-                --j;
-                t0 = 0;
-            }
-            st_release(my, kFlagInc | (unsigned long long)(prefix + agg));
-        }
-        a.tile_excl[tile * C + c] = (int32_t)prefix;
-        excl[c] = prefix;
-    };
+    // warps 0 and 1: prefixes over (warp, round) in atom order and the tile's
+    // survivor and member counts
     if (warp < 2) {
         int* cnt = warp == 0 ? cnt_s : cnt_m;
         constexpr int kPer = kMatterAtoms * kMatterWarps / 32;  // 2 entries per lane
@@ -392,12 +367,65 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_pass_kernel(const Ma
         int run = incl - tot;
 #pragma unroll
         for (int j = 0; j < kPer; ++j) { cnt[lane * kPer + j] = run; run += v[j]; }
-        if (lane == 31) look_back(warp, incl);
-    } else {
-        for (int c = tid - 62; c < C; c += kMatterThreads - 64)     // up to 128 per-loop categories
-            look_back(c, (int64_t)cnt_c[c - 2]);
+        if (lane == 31) aggv[warp] = incl;
     }
     __syncthreads();
+
+    // decoupled look-back: publish the tile's counts, then one warp scans the
+    // flags of the 32 preceding tiles at a time for the nearest published
+    // inclusive prefix (every tile between must have published its counts),
+    // and every category's thread sums that window's values
+    const int32_t my_agg = tid < C ? (tid < 2 ? aggv[tid] : cnt_c[tid - 2]) : 0;
+    if (tid < C) {
+        a.agg[tile * C + tid] = my_agg;
+        if (tile == 0) a.inc[tid] = my_agg;
+        __threadfence();
+    }
+    __syncthreads();
+    if (tid == 0) st_release(a.flags + tile, tile == 0 ? kFlagInc : kFlagAgg);
+    int64_t pre = 0;
+    if (tile > 0) {
+        int64_t jhi = tile - 1;                                 // top of the window
+        while (true) {
+            if (warp == 0) {
+                unsigned long long t0 = 0;
+                int k;
+                while (true) {
+                    const int64_t j = jhi - lane;
+                    const int f = j >= 0 ? ld_acquire(a.flags + j) : kFlagAgg;
+                    const unsigned bi = __ballot_sync(0xffffffffu, f == kFlagInc);
+                    const unsigned br = __ballot_sync(0xffffffffu, f >= kFlagAgg);
+                    k = bi ? __ffs(bi) - 1 : 32;                 // nearest inclusive prefix
+                    const unsigned need = k == 32 ? 0xffffffffu : ((1u << k) - 1u);
+                    if ((br & need) == need) break;
+                    if (t0 == 0) t0 = global_ns();
+                    else if (global_ns() - t0 > kWaitLimitNs) {
+                        if (lane == 0) report(a.err, DISCO_ETIMEOUT);
+                        k = -1;
+                        break;
+                    }
+                }
+                if (lane == 0) s_k = k;
+            }
+            __syncthreads();
+            const int k = s_k;
+            if (k < 0) break;                                   // gave up: publish anyway
+            if (tid < C) {
+                for (int q = 0; q < k; ++q) pre += __ldcg(a.agg + (jhi - q) * C + tid);
+                if (k < 32) pre += __ldcg(a.inc + (jhi - k) * C + tid);
+            }
+            if (k < 32) break;
+            jhi -= 32;
+            __syncthreads();                                    // s_k is rewritten
+        }
+    }
+    if (tid < C) {
+        if (tile > 0) a.inc[tile * C + tid] = (int32_t)(pre + my_agg);
+        excl[tid] = pre;
+        __threadfence();
+    }
+    __syncthreads();
+    if (tid == 0 && tile > 0) st_release(a.flags + tile, kFlagInc);
 
     // survivors at their final ranks, the new-index map, member records
     const unsigned ltm = (1u << lane) - 1u;
@@ -449,11 +477,11 @@ __global__ void __launch_bounds__(256) matter_tail_kernel(const MatterArgs a, in
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nl = a.nl, C = a.C;
     const int64_t t = blockIdx.x;
-    const int64_t m0 = a.tile_excl[t * C + 1];                       // this tile's member records
-    const int64_t mend = (int64_t)(a.status[t * C + 1] & kValMask);  // its inclusive count
+    const int64_t mend = a.inc[t * C + 1];                           // this tile's member records
+    const int64_t m0 = mend - a.agg[t * C + 1];
     if (t != 0 && mend == m0) return;
     // totals = the last tile's inclusive counts; loop and copy bases
-    for (int c = tid; c < C; c += 256) tot[c] = (int64_t)(a.status[(ntiles - 1) * C + c] & kValMask);
+    for (int c = tid; c < C; c += 256) tot[c] = a.inc[(ntiles - 1) * C + c];
     if (tid == 0) umask = 0ull;
     for (int i = tid; i < 2 * nl; i += 256) run[i] = 0;
     __syncthreads();
@@ -489,14 +517,16 @@ __global__ void __launch_bounds__(256) matter_tail_kernel(const MatterArgs a, in
             for (int w = 0; w < warp; ++w) { pi += wc[w][0]; pk += wc[w][1]; }
             const unsigned ltm = (1u << lane) - 1u;
             if (in) {
-                const int64_t q = lbase[l] + a.tile_excl[t * C + 2 + l] + pi + __popc(bi & ltm);
+                const int64_t q = lbase[l] + (a.inc[t * C + 2 + l] - a.agg[t * C + 2 + l]) + pi +
+                                  __popc(bi & ltm);
                 if (q < a.slab_cap) {
                     a.slab_atoms[q] = m.atom;
                     a.slab_side[q] = ((m.sides >> l) & 1ull) ? 1 : -1;
                 }
             }
             if (keep) {
-                const int64_t q = cbase[l] + a.tile_excl[t * C + 2 + nl + l] + pk + __popc(bk & ltm);
+                const int64_t q = cbase[l] + (a.inc[t * C + 2 + nl + l] - a.agg[t * C + 2 + nl + l]) + pk +
+                                  __popc(bk & ltm);
                 if (q < a.copy_cap) {
                     const disco_slab_loop& g = a.loops[l].L;
                     const double* sh = ((m.sides >> l) & 1ull) ? g.shift_pos : g.shift_neg;
@@ -727,13 +757,14 @@ int stage_loops(const disco_slab_loop* loops, int nloops, const double box[3], d
     return DISCO_OK;
 }
 
-// Bytes of the look-back words (ticket and error word first).
-size_t status_bytes(int64_t ntiles, int C) { return 16 + (size_t)ntiles * C * sizeof(unsigned long long); }
+// Bytes of the look-back flags (ticket and error word first), cleared per call.
+size_t status_bytes(int64_t ntiles) { return 16 + (size_t)ntiles * sizeof(int); }
 
 struct MatterScratch {
     unsigned char* loops;        // heads then records (sizeof(LoopStage))
-    unsigned char* status;       // status_bytes(ntiles, C)
-    int32_t* tile_excl;          // ntiles * C
+    unsigned char* status;       // status_bytes(ntiles)
+    int32_t* agg;                // ntiles * C
+    int32_t* inc;                // ntiles * C
     disco::MemberRec* members;
     int64_t member_cap;
     int64_t* totals;             // C + 1 (the last: the kernels' error word)
@@ -749,14 +780,15 @@ int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int
     a.loops = reinterpret_cast<const SlabLoopDev*>(m.loops + recs_offset(nl));
     a.nl = nl;
     a.C = 2 + 2 * nl;
-    a.status = reinterpret_cast<unsigned long long*>(m.status + 16);
+    a.flags = reinterpret_cast<int*>(m.status + 16);
     a.ticket = reinterpret_cast<unsigned int*>(m.status);
     a.err = reinterpret_cast<int*>(m.status + 4);
-    a.tile_excl = m.tile_excl;
+    a.agg = m.agg;
+    a.inc = m.inc;
     a.members = m.members;
     a.member_cap = m.member_cap;
     a.totals = m.totals;
-    e = cudaMemsetAsync(m.status, 0, status_bytes(ntiles, a.C), s);
+    e = cudaMemsetAsync(m.status, 0, status_bytes(ntiles), s);
     if (e != cudaSuccess) return cfail(e, "look-back reset");
     if (kMatterSmem > 48 * 1024) {
         e = cudaFuncSetAttribute(matter_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMatterSmem);
@@ -849,7 +881,7 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     const int64_t member_cap = std::max<int64_t>(1, std::min<int64_t>(n, slab_capacity));
     const int64_t scap = std::max<int64_t>(1, slab_capacity), ccap = std::max<int64_t>(1, copy_capacity);
 
-    DevBuf dxyz, dout, didx, dloops, dstat, dexcl, dmem, dtot, dslab, dside, dcop;
+    DevBuf dxyz, dout, didx, dloops, dstat, dagg, dmem, dtot, dslab, dside, dcop;
     const size_t nb = (size_t)n * sizeof(double);
     cudaError_t e = cudaSuccess;
     if (n > 0) {
@@ -858,8 +890,8 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
         if (e == cudaSuccess) e = cudaMalloc(&didx.p, (size_t)n * sizeof(int32_t));
     }
     if (e == cudaSuccess) e = cudaMalloc(&dloops.p, sizeof(LoopStage));
-    if (e == cudaSuccess) e = cudaMalloc(&dstat.p, status_bytes(ntiles, C));
-    if (e == cudaSuccess) e = cudaMalloc(&dexcl.p, std::max<int64_t>(1, ntiles * C) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dstat.p, status_bytes(ntiles));
+    if (e == cudaSuccess) e = cudaMalloc(&dagg.p, 2 * std::max<int64_t>(1, ntiles * C) * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&dmem.p, (size_t)member_cap * sizeof(MemberRec));
     if (e == cudaSuccess) e = cudaMalloc(&dtot.p, (size_t)(C + 1) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&dslab.p, (size_t)scap * sizeof(int32_t));
@@ -891,7 +923,8 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     MatterScratch m;
     m.loops = dloops.as<unsigned char>();
     m.status = dstat.as<unsigned char>();
-    m.tile_excl = dexcl.as<int32_t>();
+    m.agg = dagg.as<int32_t>();
+    m.inc = m.agg + std::max<int64_t>(1, ntiles * C);
     m.members = dmem.as<MemberRec>();
     m.member_cap = member_cap;
     m.totals = dtot.as<int64_t>();
@@ -992,7 +1025,7 @@ int disco_b200_finalize_resident(const double* x, const double* y, const double*
 // does, a process with a fixed memory budget) cannot let the library call
 // cudaMalloc.  disco_b200_prismatic_noalloc takes device inputs and outputs
 // from the caller and keeps its scratch (loop table, look-back words, per-tile
-// prefixes, member records, totals) in the file-scope array below: 5 MiB
+// prefixes, member records, totals) in the file-scope array below: 4 MiB
 // that every GPU loading this library holds until the process exits.
 
 namespace {
@@ -1003,13 +1036,14 @@ constexpr int64_t kNoAllocMaxMembers = int64_t(1) << 16;                // atoms
 constexpr size_t align256c(size_t v) { return (v + 255) & ~size_t(255); }
 constexpr size_t kNoAllocLoopOff = 0;
 constexpr size_t kNoAllocStatusOff = kNoAllocLoopOff + align256c(sizeof(LoopStage));
-constexpr size_t kNoAllocExclOff =
-    kNoAllocStatusOff + align256c(16 + (size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(unsigned long long));
+constexpr size_t kNoAllocAggOff = kNoAllocStatusOff + align256c(16 + (size_t)kNoAllocMaxTiles * sizeof(int));
+constexpr size_t kNoAllocIncOff =
+    kNoAllocAggOff + align256c((size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(int32_t));
 constexpr size_t kNoAllocMemberOff =
-    kNoAllocExclOff + align256c((size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(int32_t));
+    kNoAllocIncOff + align256c((size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(int32_t));
 constexpr size_t kNoAllocTotalsOff =
     kNoAllocMemberOff + align256c((size_t)kNoAllocMaxMembers * sizeof(disco::MemberRec));
-constexpr size_t kNoAllocScratchBytes = 5 * 1024 * 1024;
+constexpr size_t kNoAllocScratchBytes = 4 * 1024 * 1024;
 static_assert(kNoAllocTotalsOff + (disco::kMaxCats + 1) * sizeof(int64_t) <= kNoAllocScratchBytes,
               "no-alloc scratch layout");
 
@@ -1129,7 +1163,8 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     MatterScratch m;
     m.loops = base + kNoAllocLoopOff;
     m.status = base + kNoAllocStatusOff;
-    m.tile_excl = reinterpret_cast<int32_t*>(base + kNoAllocExclOff);
+    m.agg = reinterpret_cast<int32_t*>(base + kNoAllocAggOff);
+    m.inc = reinterpret_cast<int32_t*>(base + kNoAllocIncOff);
     m.members = reinterpret_cast<MemberRec*>(base + kNoAllocMemberOff);
     m.member_cap = member_cap;
     m.totals = reinterpret_cast<int64_t*>(base + kNoAllocTotalsOff);

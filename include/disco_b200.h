@@ -419,7 +419,7 @@ int disco_b200_prismatic(const double *x, const double *y, const double *z, int6
  * except info and counts are DEVICE pointers the caller allocated; loops,
  * box, info and counts are host memory.  Work is queued on `stream` (a
  * cudaStream_t; NULL = legacy default stream) and the call waits for it once,
- * at the end, to read the totals.  Scratch lives in a fixed 5 MiB device
+ * at the end, to read the totals.  Scratch lives in a fixed 4 MiB device
  * array inside the library (held by every GPU that loads it until the process
  * exits): at most 4 194 304 atoms, 64 prismatic loops and 65 536 atoms in
  * slabs per call, DISCO_ELIMIT beyond.  The first call on a device looks up

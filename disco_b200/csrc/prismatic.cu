@@ -40,14 +40,27 @@ struct SlabLoopDev {
     disco_slab_loop L;
     double tLo, tHi;       // slab bounds in units of d (Code/prismatic.cpp:58-59)
     double cuv, det;       // u.v and 1 - (u.v)^2 (Code/loop.cpp:327-328)
+    double inv_sp;         // 1 / d, rounded (the division's fast path)
+    double pad;
 };
 
 // ---- the predicate, FP64 round-to-nearest, reference operation order -------------------
 
-__device__ __forceinline__ double min_image(double r, double L)
+// r - L * floor(r / L + 0.5)   (Code/prismatic.cpp:31-34).  The image index
+// comes from r times the rounded 1/L unless r/L + 1/2 lies within 1e-9 of an
+// integer: the product and the exact quotient differ by under 4e-16 |r/L|
+// (|r/L| < 1e6 here), so away from that margin both give the same floor;
+// near it (or farther out) the exact quotient is taken.  The result is then
+// formed exactly as the reference forms it.
+__device__ __forceinline__ double min_image(double r, double L, double invL)
 {
-    // r - L * floor(r / L + 0.5)   (Code/prismatic.cpp:31-34)
-    return __dsub_rn(r, __dmul_rn(L, floor(__dadd_rn(__ddiv_rn(r, L), 0.5))));
+    const double q = r * invL;
+    const double h = q + 0.5;
+    const double f = floor(h);
+    const double fr = h - f;
+    const double m = (fabs(q) < 1e6 && fr > 1e-9 && fr < 1.0 - 1e-9)
+                         ? f : floor(__dadd_rn(__ddiv_rn(r, L), 0.5));
+    return __dsub_rn(r, __dmul_rn(L, m));
 }
 
 __device__ __forceinline__ double dot3_rn(double a0, double a1, double a2, double b0, double b1, double b2)
@@ -59,8 +72,14 @@ __device__ __forceinline__ double dot3_rn(double a0, double a1, double a2, doubl
 __device__ bool inside_uv_rn(const disco_slab_loop& g, double u, double v)
 {
     const double eps = 1e-9;
-    if (g.shape == DISCO_SHAPE_CIRCLE)
-        return __dsqrt_rn(__dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v))) < __dsub_rn(g.radius, eps);
+    if (g.shape == DISCO_SHAPE_CIRCLE) {
+        // sqrt(x) < y without the square root unless x is within 1e-14 of y^2
+        const double x = __dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v)), y = __dsub_rn(g.radius, eps);
+        const double y2 = y * y;
+        if (y > 0.0 && x < y2 * (1.0 - 1e-14)) return true;
+        if (y > 0.0 && x > y2 * (1.0 + 1e-14)) return false;
+        return __dsqrt_rn(x) < y;
+    }
     if (g.shape == DISCO_SHAPE_POLYGON) {
         const int N = g.n_poly;
         bool inner = true;
@@ -90,20 +109,33 @@ __device__ bool inside_uv_rn(const disco_slab_loop& g, double u, double v)
 }
 
 // Slab membership of one atom (Code/prismatic.cpp:61-72); side = sign of s.
+// Every value that decides it is the reference's, rounded as the reference
+// rounds it; divisions are skipped only where the decision provably does not
+// depend on them: t = s / d against the slab bounds from s times the rounded
+// 1/d unless that lies within 1e-9 planes of a bound, and the in-plane
+// coordinates' division by det = 1 - (u.v)^2 when det is exactly 1.
 __device__ __noinline__ bool slab_member(const SlabLoopDev& S, double x, double y, double z,
-                                            double Lx, double Ly, double Lz, bool& pos_side)
+                                         double Lx, double Ly, double Lz, double iLx, double iLy, double iLz,
+                                         bool& pos_side)
 {
     const disco_slab_loop& g = S.L;
-    const double r0 = min_image(__dsub_rn(x, g.c[0]), Lx);
-    const double r1 = min_image(__dsub_rn(y, g.c[1]), Ly);
-    const double r2 = min_image(__dsub_rn(z, g.c[2]), Lz);
+    const double r0 = min_image(__dsub_rn(x, g.c[0]), Lx, iLx);
+    const double r1 = min_image(__dsub_rn(y, g.c[1]), Ly, iLy);
+    const double r2 = min_image(__dsub_rn(z, g.c[2]), Lz, iLz);
     const double s = dot3_rn(r0, r1, r2, g.n[0], g.n[1], g.n[2]);
-    const double t = __ddiv_rn(s, g.spacing);
-    if (t < S.tLo || t >= S.tHi) return false;
+    const double tf = s * S.inv_sp;
+    const double dlt = 1e-9 * (fabs(tf) + 1.0);
+    if (tf < S.tLo - dlt || tf >= S.tHi + dlt) return false;
+    if (!(tf >= S.tLo + dlt && tf < S.tHi - dlt)) {
+        const double t = __ddiv_rn(s, g.spacing);
+        if (t < S.tLo || t >= S.tHi) return false;
+    }
     const double ru = dot3_rn(r0, r1, r2, g.u[0], g.u[1], g.u[2]);
     const double rv = dot3_rn(r0, r1, r2, g.v[0], g.v[1], g.v[2]);
-    const double uu = __ddiv_rn(__dsub_rn(ru, __dmul_rn(S.cuv, rv)), S.det);
-    const double vv = __ddiv_rn(__dsub_rn(rv, __dmul_rn(S.cuv, ru)), S.det);
+    const double nu = __dsub_rn(ru, __dmul_rn(S.cuv, rv));
+    const double nv = __dsub_rn(rv, __dmul_rn(S.cuv, ru));
+    const double uu = S.det == 1.0 ? nu : __ddiv_rn(nu, S.det);
+    const double vv = S.det == 1.0 ? nv : __ddiv_rn(nv, S.det);
     if (!inside_uv_rn(g, uu, vv)) return false;
     pos_side = s > 0.;
     return true;
@@ -136,6 +168,7 @@ constexpr int kMatterAtoms = 8;                                // per thread
 constexpr int kMatterTile = kMatterThreads * kMatterAtoms;     // 2048 atoms per tile
 constexpr int kMatterWarps = kMatterThreads / 32;
 constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // look-back categories
+constexpr int kWarpQueue = 128;                                // exact tests queued per warp
 constexpr size_t kMatterSmem = 2 * kMatterTile * sizeof(uint64_t); // masks and sides of a tile
 
 // Tile flags of the look-back: 0 not yet published, 1 the tile's counts
@@ -153,6 +186,7 @@ struct MatterArgs {
     double Lx, Ly, Lz;
     float iLx, iLy, iLz;          // 1 / box lengths in FP32 (the pre-test only)
     int32_t pad_;
+    double idLx, idLy, idLz;      // 1 / box lengths, rounded (the exact test's fast path)
     int* flags;                   // [ntiles] look-back flags, zeroed per call
     unsigned int* ticket;         // tile counter, zeroed per call
     int32_t* agg;                 // [ntiles][C] the tile's counts
@@ -222,14 +256,11 @@ __device__ __forceinline__ double periodic_gap(double lo, double hi, double c, d
     return fmax(0.0, d - 1e-9 * L - 1e-6);
 }
 
-// Membership of one atom over the loops in `cand` (bits of loops whose slab
-// the tile can reach): the FP32 pre-test, then the exact FP64 test in loop order.
-__device__ __forceinline__ void atom_masks(const SlabHead* sh, const SlabLoopDev* sl, uint64_t cand, double x,
-                                           double y, double z, const MatterArgs& a, uint64_t& mask,
-                                           uint64_t& sides, bool& removed)
+// The loops among `cand` (loops whose slab can reach the atom's warp) that the
+// FP32 pre-test cannot exclude for this atom: its exact-test candidates.
+__device__ __forceinline__ uint64_t pretest(const SlabHead* sh, uint64_t cand, double x, double y, double z,
+                                            const MatterArgs& a)
 {
-    mask = 0; sides = 0; removed = false;
-    if (!cand) return;
     const float L[3] = { (float)a.Lx, (float)a.Ly, (float)a.Lz };
     const float iL[3] = { a.iLx, a.iLy, a.iLz };
     const float p[3] = { (float)x, (float)y, (float)z };
@@ -238,16 +269,7 @@ __device__ __forceinline__ void atom_masks(const SlabHead* sh, const SlabLoopDev
         const int l = __ffsll((long long)c) - 1;
         if (!clearly_outside(sh[l], p, L, iL)) c2 |= 1ull << l;
     }
-    while (c2) {
-        const int l = __ffsll((long long)c2) - 1;
-        c2 &= c2 - 1;
-        bool ps = false;
-        if (slab_member(sl[l], x, y, z, a.Lx, a.Ly, a.Lz, ps)) {
-            mask |= 1ull << l;
-            if (ps) sides |= 1ull << l;
-            if (sh[l].type == DISCO_MATTER_VACANCY) removed = true;
-        }
-    }
+    return c2;
 }
 
 // The matter step's single pass over the atoms.  Each CTA takes the next tile
@@ -275,6 +297,8 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_pass_kernel(const Ma
     __shared__ int64_t excl[kMaxCats];
     __shared__ int aggv[2];
     __shared__ int s_k;
+    __shared__ int wq[kMatterWarps][kWarpQueue];                // per warp: (slot, loop) pairs to test
+    __shared__ int wq_n[kMatterWarps];
     __shared__ unsigned long long vac_s;
     __shared__ int tile_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -329,18 +353,54 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_pass_kernel(const Ma
     __syncthreads();                                        // vac_s
     const uint64_t vac = vac_s;
 
-    // every atom's mask, once; counts per (warp, round) and per loop
+    // every atom's mask, once: the FP32 pre-test per atom, its candidate
+    // (atom, loop) pairs queued per warp, the exact FP64 tests of the queue
+    // spread over the warp's lanes (one latency chain per 32 pairs rather than
+    // one per round and loop), then the counts per (warp, round) and per loop
     const int wt = warp * (32 * kMatterAtoms);              // the warp's first atom in the tile
+    if (lane == 0) wq_n[warp] = 0;
+    __syncwarp();
 #pragma unroll 1
     for (int r = 0; r < kMatterAtoms; ++r) {
         const int64_t i = wbase + r * 32 + lane;
-        const bool valid = i < a.n;
-        uint64_t mask = 0, sides = 0;
-        bool removed = false;
-        if (valid && wmask) atom_masks(sh, a.loops, wmask, a.x[i], a.y[i], a.z[i], a, mask, sides, removed);
-        smask[wt + r * 32 + lane] = mask;
-        ssides[wt + r * 32 + lane] = sides;
-        const unsigned bs = __ballot_sync(0xffffffffu, valid && !removed);
+        uint64_t cand = 0;
+        if (i < a.n && wmask) cand = pretest(sh, wmask, a.x[i], a.y[i], a.z[i], a);
+        smask[wt + r * 32 + lane] = 0;
+        ssides[wt + r * 32 + lane] = 0;
+        for (uint64_t c = cand; c; c &= c - 1) {
+            const int l = __ffsll((long long)c) - 1;
+            const int q = atomicAdd(&wq_n[warp], 1);
+            if (q < kWarpQueue) {
+                wq[warp][q] = (r * 32 + lane) | (l << 16);
+            } else {                                         // a full queue: test here
+                bool ps = false;
+                if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy, a.idLz, ps)) {
+                    smask[wt + r * 32 + lane] |= 1ull << l;
+                    if (ps) ssides[wt + r * 32 + lane] |= 1ull << l;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    {
+        const int nq = min(wq_n[warp], kWarpQueue);
+        for (int q = lane; q < nq; q += 32) {
+            const int slot = wq[warp][q] & 0xffff, l = wq[warp][q] >> 16;
+            const int64_t i = wbase + slot;
+            bool ps = false;
+            if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy, a.idLz, ps)) {
+                atomicOr(reinterpret_cast<unsigned long long*>(&smask[wt + slot]), 1ull << l);
+                if (ps) atomicOr(reinterpret_cast<unsigned long long*>(&ssides[wt + slot]), 1ull << l);
+            }
+        }
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int r = 0; r < kMatterAtoms; ++r) {
+        const int64_t i = wbase + r * 32 + lane;
+        const uint64_t mask = smask[wt + r * 32 + lane];
+        const bool removed = (mask & vac) != 0;
+        const unsigned bs = __ballot_sync(0xffffffffu, i < a.n && !removed);
         const unsigned bm = __ballot_sync(0xffffffffu, mask != 0);
         if (lane == 0) { cnt_s[warp * kMatterAtoms + r] = __popc(bs); cnt_m[warp * kMatterAtoms + r] = __popc(bm); }
         for (uint64_t m = mask; m; m &= m - 1) {             // members are rare
@@ -477,6 +537,7 @@ __global__ void __launch_bounds__(256) matter_tail_kernel(const MatterArgs a, in
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nl = a.nl, C = a.C;
     const int64_t t = blockIdx.x;
+    if (tid == 0) a.flags[t] = 0;            // cleared for the next call (the pass is over)
     const int64_t mend = a.inc[t * C + 1];                           // this tile's member records
     const int64_t m0 = mend - a.agg[t * C + 1];
     if (t != 0 && mend == m0) return;
@@ -494,6 +555,8 @@ __global__ void __launch_bounds__(256) matter_tail_kernel(const MatterArgs a, in
         if (t == 0) {
             for (int c = 0; c < C; ++c) a.totals[c] = tot[c];
             a.totals[C] = *a.err;                              // the pass's error word
+            *a.err = 0;                                        // ticket and error word cleared
+            *a.ticket = 0;                                     // for the next call
         }
     }
     __syncthreads();
@@ -633,6 +696,7 @@ int slab_loop_record(const disco_slab_loop& g, const double box[3], disco_slab_i
     const double c = g.u[0] * g.v[0] + g.u[1] * g.v[1] + g.u[2] * g.v[2];
     d.cuv = c;
     d.det = 1.0 - c * c;
+    d.inv_sp = 1.0 / g.spacing;
 
     std::memset(&h, 0, sizeof(h));
     h.cx = g.c[0]; h.cy = g.c[1]; h.cz = g.c[2];
@@ -772,7 +836,8 @@ struct MatterScratch {
 
 // Queues the matter step on stream s after stage_loops (no host wait): the
 // look-back words cleared, the single pass, the tail.
-int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int64_t ntiles, cudaStream_t s)
+int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int64_t ntiles, cudaStream_t s,
+                 size_t clear_bytes)
 {
     using namespace disco;
     cudaError_t e = cudaSuccess;
@@ -788,8 +853,13 @@ int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int
     a.members = m.members;
     a.member_cap = m.member_cap;
     a.totals = m.totals;
-    e = cudaMemsetAsync(m.status, 0, status_bytes(ntiles), s);
-    if (e != cudaSuccess) return cfail(e, "look-back reset");
+    // the tail of every completed call leaves the flags, ticket and error word
+    // at zero; a caller that cannot rely on that (fresh memory, a call that
+    // failed half-way) clears them here
+    if (clear_bytes) {
+        e = cudaMemsetAsync(m.status, 0, clear_bytes, s);
+        if (e != cudaSuccess) return cfail(e, "look-back reset");
+    }
     if (kMatterSmem > 48 * 1024) {
         e = cudaFuncSetAttribute(matter_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMatterSmem);
         if (e != cudaSuccess) return cfail(e, "matter step shared memory");
@@ -913,6 +983,7 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     a.n = n;
     a.Lx = box[0]; a.Ly = box[1]; a.Lz = box[2];
     a.iLx = (float)(1.0 / box[0]); a.iLy = (float)(1.0 / box[1]); a.iLz = (float)(1.0 / box[2]);
+    a.idLx = 1.0 / box[0]; a.idLy = 1.0 / box[1]; a.idLz = 1.0 / box[2];
     a.xo = dout.as<double>(); a.yo = a.xo + n; a.zo = a.xo + 2 * n;
     a.new_index = didx.as<int32_t>();
     a.slab_atoms = dslab.as<int32_t>();
@@ -928,7 +999,7 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     m.members = dmem.as<MemberRec>();
     m.member_cap = member_cap;
     m.totals = dtot.as<int64_t>();
-    st = matter_queue(a, m, nl, ntiles, nullptr);
+    st = matter_queue(a, m, nl, ntiles, nullptr, status_bytes(ntiles));
     if (st) return st;
     int64_t tot[kMaxCats + 1];
     e = cudaMemcpy(tot, m.totals, (size_t)(C + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost);
@@ -1053,6 +1124,7 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_addr[kMaxDevices] = {};
 unsigned long long g_noalloc_ctx[kMaxDevices] = {};
+bool g_noalloc_dirty[kMaxDevices] = {};     // the look-back flags may not be zero
 
 using CtxGetCurrentFn = CUresult (*)(CUcontext*);
 using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
@@ -1087,7 +1159,7 @@ unsigned long long current_context_id()
 // looked up with that device current and cached with the identifier of the
 // context it belongs to; a new context on that device (after a device reset,
 // which reloads the module) gets a fresh lookup.
-int noalloc_scratch(unsigned char** out, unsigned long long* ctx_out)
+int noalloc_scratch(unsigned char** out, unsigned long long* ctx_out, int* dev_out)
 {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -1104,10 +1176,22 @@ int noalloc_scratch(unsigned char** out, unsigned long long* ctx_out)
         if (e != cudaSuccess || !p) return cfail(e, "cudaGetSymbolAddress of the scratch array");
         g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
         g_noalloc_ctx[dev] = ctx;
+        g_noalloc_dirty[dev] = true;
     }
+    *dev_out = dev;
     *out = g_noalloc_addr[dev];
     *ctx_out = ctx;
     return DISCO_OK;
+}
+
+// Reads (and with `take`, clears) or sets a device's dirty flag.
+bool noalloc_dirty(int dev, bool take, bool set)
+{
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    const bool was = g_noalloc_dirty[dev];
+    if (take) g_noalloc_dirty[dev] = false;
+    if (set) g_noalloc_dirty[dev] = true;
+    return was;
 }
 
 } // namespace
@@ -1136,7 +1220,8 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned char* base = nullptr;
     unsigned long long ctx = 0;
-    int st = noalloc_scratch(&base, &ctx);
+    int dev = 0;
+    int st = noalloc_scratch(&base, &ctx, &dev);
     if (st) return st;
 
     int act_index[kMaxSlabLoops];
@@ -1153,6 +1238,7 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     a.n = n;
     a.Lx = box[0]; a.Ly = box[1]; a.Lz = box[2];
     a.iLx = (float)(1.0 / box[0]); a.iLy = (float)(1.0 / box[1]); a.iLz = (float)(1.0 / box[2]);
+    a.idLx = 1.0 / box[0]; a.idLy = 1.0 / box[1]; a.idLz = 1.0 / box[2];
     a.xo = x_out; a.yo = y_out; a.zo = z_out;
     a.new_index = new_index;
     a.slab_atoms = slab_atoms;
@@ -1168,12 +1254,13 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     m.members = reinterpret_cast<MemberRec*>(base + kNoAllocMemberOff);
     m.member_cap = member_cap;
     m.totals = reinterpret_cast<int64_t*>(base + kNoAllocTotalsOff);
-    st = matter_queue(a, m, nl, ntiles, s);
-    if (st) { stage_cache_drop(); return st; }
+    const bool dirty = noalloc_dirty(dev, true, false);
+    st = matter_queue(a, m, nl, ntiles, s, dirty ? status_bytes(kNoAllocMaxTiles) : 0);
+    if (st) { stage_cache_drop(); noalloc_dirty(dev, false, true); return st; }
     int64_t tot[kMaxCats + 1];
     cudaError_t e = cudaMemcpyAsync(tot, m.totals, (size_t)(C + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) { stage_cache_drop(); return cfail(e, "prismatic totals"); }
+    if (e != cudaSuccess) { stage_cache_drop(); noalloc_dirty(dev, false, true); return cfail(e, "prismatic totals"); }
     st = matter_finish(tot, nl, act_index, nloops, info, slab_capacity, copy_capacity, member_cap, counts);
     if (st == DISCO_ELIMIT && tot[1] > member_cap && counts[1] <= slab_capacity && counts[2] <= copy_capacity)
         return efail(DISCO_ELIMIT, "disco_b200_prismatic_noalloc takes at most 65536 atoms in slabs "

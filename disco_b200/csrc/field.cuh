@@ -84,7 +84,8 @@ struct alignas(16) LineSegF {
     float tx, ty, tz;        // unit tangent
     float wx, wy, wz;        // b x t
     float nx, ny, nz;        // (start - centre) x (end - centre)
-    float pad0, pad1, pad2;  // 64 B
+    float hl2;               // length^2 / 2
+    float pad1, pad2;        // 64 B
 };
 static_assert(sizeof(LinePieceF) == 80 && sizeof(LineSegF) == 64, "fp32 line table layout");
 

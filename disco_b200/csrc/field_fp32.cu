@@ -97,6 +97,7 @@ int build_table_fp32(const disco_loop* loops, int nloops, int kind, double nu, H
                     f.tx = (float)sg.tx; f.ty = (float)sg.ty; f.tz = (float)sg.tz;
                     f.wx = (float)sg.wx; f.wy = (float)sg.wy; f.wz = (float)sg.wz;      // cK w
                     f.nx = (float)sg.nx; f.ny = (float)sg.ny; f.nz = (float)sg.nz;
+                    f.hl2 = (float)sg.hl2;
                     recs.push_back(f);
                 }
                 p64.push_back(q);

@@ -101,7 +101,7 @@ __device__ __forceinline__ void line_piece_fp32(const LinePieceF& pc, const Line
         const float ilb = rsqrt_ftz(lb2);
         const float lb = lb2 * ilb;
         const float eb = ex * bx + ey * by + ez * bz;
-        const float den = fmaf(ea, lb, fmaf(eb, la, fmaf(la, lb, ax * bx + ay * by + az * bz)));
+        const float den = fmaf(ea, lb, fmaf(eb, la, fmaf(la, lb, fmaf(0.5f, la2 + lb2, -s.hl2))));   // a.b
         const float num = ex * s.nx + ey * s.ny + ez * s.nz;
         const float nzr = zr * den - zi * num;
         zi = zr * num + zi * den;

@@ -521,7 +521,7 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_pass_kernel(const Ma
 }
 
 // The slab entries and the interstitial copies, from the member records of
-// one tile (CTA t <-> tile t, after the pass has finished): entry of loop l
+// each tile (tiles spread over the CTAs, after the pass): entry of loop l
 // at loop base + the tile's exclusive count of loop l + its rank among the
 // tile's members in l (ascending atom order, Code/prismatic.cpp:61-72); a copy
 // of an interstitial loop's entry whose atom survives at copy base + the tile's
@@ -536,15 +536,8 @@ __global__ void __launch_bounds__(256) matter_tail_kernel(const MatterArgs a, in
     __shared__ unsigned long long umask;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nl = a.nl, C = a.C;
-    const int64_t t = blockIdx.x;
-    if (tid == 0) a.flags[t] = 0;            // cleared for the next call (the pass is over)
-    const int64_t mend = a.inc[t * C + 1];                           // this tile's member records
-    const int64_t m0 = mend - a.agg[t * C + 1];
-    if (t != 0 && mend == m0) return;
     // totals = the last tile's inclusive counts; loop and copy bases
     for (int c = tid; c < C; c += 256) tot[c] = a.inc[(ntiles - 1) * C + c];
-    if (tid == 0) umask = 0ull;
-    for (int i = tid; i < 2 * nl; i += 256) run[i] = 0;
     __syncthreads();
     if (tid == 0) {
         int64_t sb = 0, cb = 0;
@@ -552,62 +545,73 @@ __global__ void __launch_bounds__(256) matter_tail_kernel(const MatterArgs a, in
             lbase[l] = sb; sb += tot[2 + l];
             cbase[l] = cb; cb += tot[2 + nl + l];
         }
-        if (t == 0) {
+        if (blockIdx.x == 0) {
             for (int c = 0; c < C; ++c) a.totals[c] = tot[c];
             a.totals[C] = *a.err;                              // the pass's error word
             *a.err = 0;                                        // ticket and error word cleared
             *a.ticket = 0;                                     // for the next call
         }
     }
-    __syncthreads();
-    for (int64_t e0 = m0; e0 < mend; e0 += 256) {
-        const int64_t e = e0 + tid;
-        MemberRec m;
-        m.atom = 0; m.removed = 1; m.mask = 0; m.sides = 0;
-        if (e < mend && e < a.member_cap) m = a.members[e];
-        if (m.mask) atomicOr(&umask, m.mask);
+    // this CTA's tiles (grid-stride): each tile's flag cleared for the next
+    // call (the pass is over), its member records turned into entries
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        if (tid == 0) a.flags[t] = 0;
+        const int64_t mend = a.inc[t * C + 1];                           // this tile's member records
+        const int64_t m0 = mend - a.agg[t * C + 1];
+        if (mend == m0) continue;
+        __syncthreads();                                    // run / umask of the previous tile
+        if (tid == 0) umask = 0ull;
+        for (int i = tid; i < 2 * nl; i += 256) run[i] = 0;
         __syncthreads();
-        const uint64_t um = umask;
-        for (uint64_t u = um; u; u &= u - 1) {
-            const int l = __ffsll((long long)u) - 1;
-            const bool in = (m.mask >> l) & 1ull;
-            const bool keep = in && !m.removed && a.heads[l].type == DISCO_MATTER_INTERSTITIAL;
-            const unsigned bi = __ballot_sync(0xffffffffu, in);
-            const unsigned bk = __ballot_sync(0xffffffffu, keep);
-            if (lane == 0) { wc[warp][0] = __popc(bi); wc[warp][1] = __popc(bk); }
+        for (int64_t e0 = m0; e0 < mend; e0 += 256) {
+            const int64_t e = e0 + tid;
+            MemberRec m;
+            m.atom = 0; m.removed = 1; m.mask = 0; m.sides = 0;
+            if (e < mend && e < a.member_cap) m = a.members[e];
+            if (m.mask) atomicOr(&umask, m.mask);
             __syncthreads();
-            int pi = run[l], pk = run[nl + l];
-            for (int w = 0; w < warp; ++w) { pi += wc[w][0]; pk += wc[w][1]; }
-            const unsigned ltm = (1u << lane) - 1u;
-            if (in) {
-                const int64_t q = lbase[l] + (a.inc[t * C + 2 + l] - a.agg[t * C + 2 + l]) + pi +
-                                  __popc(bi & ltm);
-                if (q < a.slab_cap) {
-                    a.slab_atoms[q] = m.atom;
-                    a.slab_side[q] = ((m.sides >> l) & 1ull) ? 1 : -1;
+            const uint64_t um = umask;
+            for (uint64_t u = um; u; u &= u - 1) {
+                const int l = __ffsll((long long)u) - 1;
+                const bool in = (m.mask >> l) & 1ull;
+                const bool keep = in && !m.removed && a.heads[l].type == DISCO_MATTER_INTERSTITIAL;
+                const unsigned bi = __ballot_sync(0xffffffffu, in);
+                const unsigned bk = __ballot_sync(0xffffffffu, keep);
+                if (lane == 0) { wc[warp][0] = __popc(bi); wc[warp][1] = __popc(bk); }
+                __syncthreads();
+                int pi = run[l], pk = run[nl + l];
+                for (int w = 0; w < warp; ++w) { pi += wc[w][0]; pk += wc[w][1]; }
+                const unsigned ltm = (1u << lane) - 1u;
+                if (in) {
+                    const int64_t q = lbase[l] + (a.inc[t * C + 2 + l] - a.agg[t * C + 2 + l]) + pi +
+                                      __popc(bi & ltm);
+                    if (q < a.slab_cap) {
+                        a.slab_atoms[q] = m.atom;
+                        a.slab_side[q] = ((m.sides >> l) & 1ull) ? 1 : -1;
+                    }
                 }
-            }
-            if (keep) {
-                const int64_t q = cbase[l] + (a.inc[t * C + 2 + nl + l] - a.agg[t * C + 2 + nl + l]) + pk +
-                                  __popc(bk & ltm);
-                if (q < a.copy_cap) {
-                    const disco_slab_loop& g = a.loops[l].L;
-                    const double* sh = ((m.sides >> l) & 1ull) ? g.shift_pos : g.shift_neg;
-                    disco_copy cp;
-                    cp.atom = a.new_index[m.atom];
-                    cp.reserved = 0;
-                    cp.shift[0] = sh[0]; cp.shift[1] = sh[1]; cp.shift[2] = sh[2];
-                    a.copies[q] = cp;
+                if (keep) {
+                    const int64_t q = cbase[l] + (a.inc[t * C + 2 + nl + l] - a.agg[t * C + 2 + nl + l]) + pk +
+                                      __popc(bk & ltm);
+                    if (q < a.copy_cap) {
+                        const disco_slab_loop& g = a.loops[l].L;
+                        const double* sh = ((m.sides >> l) & 1ull) ? g.shift_pos : g.shift_neg;
+                        disco_copy cp;
+                        cp.atom = a.new_index[m.atom];
+                        cp.reserved = 0;
+                        cp.shift[0] = sh[0]; cp.shift[1] = sh[1]; cp.shift[2] = sh[2];
+                        a.copies[q] = cp;
+                    }
                 }
+                __syncthreads();
+                if (tid == 0) {
+                    for (int w = 0; w < 8; ++w) { run[l] += wc[w][0]; run[nl + l] += wc[w][1]; }
+                }
+                __syncthreads();
             }
-            __syncthreads();
-            if (tid == 0) {
-                for (int w = 0; w < 8; ++w) { run[l] += wc[w][0]; run[nl + l] += wc[w][1]; }
-            }
+            if (tid == 0) umask = 0ull;
             __syncthreads();
         }
-        if (tid == 0) umask = 0ull;
-        __syncthreads();
     }
 }
 // Code/main.cpp:733-743 + 797-818: copies appended with u(src) + shift, then
@@ -866,7 +870,7 @@ int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int
     }
     if (ntiles > 0) {
         matter_pass_kernel<<<(unsigned)ntiles, kMatterThreads, kMatterSmem, s>>>(a);
-        matter_tail_kernel<<<(unsigned)ntiles, 256, 0, s>>>(a, ntiles);
+        matter_tail_kernel<<<(unsigned)std::min<int64_t>(ntiles, 512), 256, 0, s>>>(a, ntiles);
     } else {
         e = cudaMemsetAsync(m.totals, 0, (size_t)(a.C + 1) * sizeof(int64_t), s);
         if (e != cudaSuccess) return cfail(e, "totals reset");

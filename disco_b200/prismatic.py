@@ -119,7 +119,7 @@ def _main():
     torch.cuda.synchronize()
     t = e0.elapsed_time(e1) * 1e-3 / a.reps
     print(f"matter step: {n} atoms, {counts[0]} survivors, {counts[1]} slab atoms, {counts[2]} copies: "
-          f"{t * 1e3:.3f} ms per call, {76.0 * n / t / 1e9:.0f} GB/s of algorithmic bytes (76 B/atom)")
+          f"{t * 1e3:.3f} ms per call, {52.0 * n / t / 1e9:.0f} GB/s of algorithmic bytes (52 B/atom)")
 
 
 if __name__ == "__main__":

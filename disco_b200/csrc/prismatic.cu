@@ -8,17 +8,14 @@
 // contract-off oracle, and the oracle's margin report shows that the
 // reference's own contracted build selects the same sets.
 //
-// Stream compaction, order-preserving, in three passes over tiles of 2048
-// atoms (8 rounds of 256):
-//   count    per tile and category (survivors, and the slab of every loop),
-//            warp ballots + shared-memory counters;
-//   scan     one CTA: exclusive scan over tiles per category, per-loop bases;
-//   scatter  the predicate again (cheaper than storing it), ranks from warp
-//            ballots and a per-round scan over the 8 warps; survivors are
-//            compacted (x, y, z and the new-index map) and slab entries
-//            written at base + tile offset + rank, i.e. ascending atom order.
-// A fourth single-CTA pass gathers the interstitial copies in loop order then
-// slab order, drops those of removed atoms and renumbers their sources.
+// The step is one cooperative kernel (matter_kernel): a first phase computes
+// every atom's slab mask once (bounding-box culling per 128-atom segment, an
+// FP32 pre-test, the exact FP64 predicate for the rest) and counts per CTA;
+// after a grid barrier the CTAs' counts are scanned per category; after a
+// second barrier the survivors are compacted in order (x, y, z and the
+// new-index map; the positions come back from L2) and the slab entries and
+// interstitial copies written in loop order, then atom order, with copies of
+// removed atoms dropped and their sources renumbered.
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
@@ -164,17 +161,19 @@ struct MemberRec {
 };
 
 constexpr int kMatterThreads = 256;
-constexpr int kMatterAtoms = 8;                                // per thread
-constexpr int kMatterTile = kMatterThreads * kMatterAtoms;     // 2048 atoms per tile
 constexpr int kMatterWarps = kMatterThreads / 32;
-constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // look-back categories
+constexpr int kSegRounds = 4;                                  // rounds of 32 atoms per segment
+constexpr int kSegAtoms = 32 * kSegRounds;                     // 128 atoms: one warp's unit of work
+constexpr int kChunkSegs = 32;                                 // segments per chunk of the second phase
+constexpr int kSegRow = 2 * kMaxSlabLoops;                     // per-loop slab and copy counts of a segment
+constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // categories counted per CTA
 constexpr int kWarpQueue = 128;                                // exact tests queued per warp
-constexpr size_t kMatterSmem = 2 * kMatterTile * sizeof(uint64_t); // masks and sides of a tile
-
-// Tile flags of the look-back: 0 not yet published, 1 the tile's counts
-// (agg) are published, 2 its inclusive prefixes (inc) are too.
-constexpr int kFlagAgg = 1;
-constexpr int kFlagInc = 2;
+constexpr int kMaxGrid = 8 * 148;                              // CTAs of one call at most
+// dynamic shared memory: per warp the masks and sides of its segment (first
+// phase), then the per-loop counts of a chunk's segments (second phase)
+constexpr size_t kMatterSmem = kMatterWarps * 2 * kSegAtoms * sizeof(uint64_t);
+static_assert(kChunkSegs * kSegRow * sizeof(int) <= kMatterSmem, "chunk counts fit the mask buffer");
+static_assert(kChunkSegs % kMatterWarps == 0, "whole rows of segments per chunk");
 
 struct MatterArgs {
     const double *x, *y, *z;
@@ -185,12 +184,16 @@ struct MatterArgs {
                                   // loop l (2 + l), kept copies of loop l (2 + nl + l)
     double Lx, Ly, Lz;
     float iLx, iLy, iLz;          // 1 / box lengths in FP32 (the pre-test only)
-    int32_t pad_;
+    int32_t G;                    // CTAs, all resident at once (cooperative launch)
     double idLx, idLy, idLz;      // 1 / box lengths, rounded (the exact test's fast path)
-    int* flags;                   // [ntiles] look-back flags, zeroed per call
-    unsigned int* ticket;         // tile counter, zeroed per call
-    int32_t* agg;                 // [ntiles][C] the tile's counts
-    int32_t* inc;                 // [ntiles][C] inclusive prefixes (exclusive = inc - agg)
+    int64_t S;                    // segments of kSegAtoms atoms
+    int32_t* seg_removed;         // [S] atoms a vacancy slab removes
+    int32_t* seg_members;         // [S] slab-member atoms
+    int32_t* seg_off;             // [S] first member record of the segment
+    int32_t* cta_tot;             // [G][C] counts per CTA
+    int32_t* cta_pre;             // [G][C] exclusive prefixes over the CTAs
+    unsigned int* ctl;            // [4] barrier arrivals, exits, member records taken, error word;
+                                  // zero at entry, left zero by the last CTA to leave
     MemberRec* members;
     int64_t member_cap;
     double *xo, *yo, *zo;
@@ -200,20 +203,63 @@ struct MatterArgs {
     int64_t slab_cap;
     disco_copy* copies;
     int64_t copy_cap;
-    int64_t* totals;              // [C] category totals (written by the tail)
-    int* err;
+    int64_t* totals;              // [C + 1] category totals, then the error word
 };
 
-__device__ __forceinline__ void st_release(int* p, int v)
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
 {
-    asm volatile("st.release.gpu.global.s32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
 }
 
-__device__ __forceinline__ int ld_acquire(const int* p)
+// L2 policies: the first phase's reads of the positions stay in L2 for the
+// second phase's (evict-last); the second phase reads them for the last time
+// (evict-first).  The positions are never written during the kernel, so these
+// loads carry no ordering constraint.
+__device__ __forceinline__ uint64_t l2_policy_keep()
 {
-    int v;
-    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ uint64_t l2_policy_last_use()
+{
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ double ld_hint(const double* p, uint64_t pol)
+{
+    double v;
+    asm("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
     return v;
+}
+
+// All CTAs of the launch arrive, then wait until `target` arrivals are
+// counted (the launch is cooperative, so every CTA is resident).  Bounded: a
+// wait that sees no progress for 2 s records DISCO_ETIMEOUT and goes on.
+__device__ __forceinline__ void grid_sync(unsigned* arrive, unsigned target, int* err)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(arrive, 1u);
+        unsigned long long t0 = 0;
+        while (ld_acquire_u32(arrive) < target) {
+            if (t0 == 0) {
+                t0 = global_ns();
+            } else if (global_ns() - t0 > kWaitLimitNs) {
+                report(err, DISCO_ETIMEOUT);
+                break;
+            }
+            __nanosleep(32);
+        }
+        __threadfence();
+    }
+    __syncthreads();
 }
 
 // Cheap pre-test in FP32: true only if the atom's t is outside [tLo, tHi) by
@@ -272,345 +318,440 @@ __device__ __forceinline__ uint64_t pretest(const SlabHead* sh, uint64_t cand, d
     return c2;
 }
 
-// The matter step's single pass over the atoms.  Each CTA takes the next tile
-// of 2048 atoms (a ticket, so that every tile it looks back on belongs to a
-// CTA already running); each warp owns 256 consecutive atoms of it (8 rounds
-// of 32, coalesced), reads them once, takes their bounding box and skips every
-// loop whose slab cannot reach it, and computes each atom's slab mask once
-// (kept in shared memory for the ranked writes).  Per category the tile's
-// count is published and its exclusive prefix obtained by decoupled
-// look-back over the preceding tiles' published counts; survivors (x, y, z,
-// new index) and the slab members' records are then written at their final
-// ranks.  Bounded waits: a look-back that finds no count for 2 s records
-// DISCO_ETIMEOUT and publishes anyway, so no tile waits forever.
-// Dynamic shared memory: kMatterTile masks and sides (32 KB); four CTAs per
-// SM, so that one CTA's barriers and look-back overlap the others' loads.
-__global__ void __launch_bounds__(kMatterThreads, 4) matter_pass_kernel(const MatterArgs a)
+// Survivors of one segment at their final ranks (x, y, z and the new-index
+// map); `sb` = survivors before the segment.  A segment with removed atoms
+// reads its member records for the removed ones' positions.
+__device__ __forceinline__ void copy_segment(const MatterArgs& a, int64_t s, int64_t sb, int srem, int m, int off,
+                                             uint64_t pol, int lane)
+{
+    const int64_t i0 = s * kSegAtoms;
+    unsigned rb[kSegRounds];
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) rb[r] = 0u;
+    if (srem > 0 && (int64_t)off + m <= a.member_cap) {
+        for (int e0 = 0; e0 < m; e0 += 32) {
+            const int e = e0 + lane;
+            unsigned li = 0xffffffffu;
+            if (e < m) {
+                const MemberRec* rec = a.members + off + e;
+                if (__ldcg(&rec->removed)) li = (unsigned)(__ldcg(&rec->atom) - i0);
+            }
+#pragma unroll
+            for (int r = 0; r < kSegRounds; ++r)
+                rb[r] |= __reduce_or_sync(0xffffffffu, (li >> 5) == (unsigned)r ? 1u << (li & 31u) : 0u);
+        }
+    }
+    double px[kSegRounds], py[kSegRounds], pz[kSegRounds];
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) {
+        const int64_t i = i0 + r * 32 + lane;
+        px[r] = py[r] = pz[r] = 0.0;
+        if (i < a.n) { px[r] = ld_hint(a.x + i, pol); py[r] = ld_hint(a.y + i, pol); pz[r] = ld_hint(a.z + i, pol); }
+    }
+    const unsigned ltm = (1u << lane) - 1u;
+    int before = 0;
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) {
+        const int64_t i = i0 + r * 32 + lane;
+        if (i < a.n) {
+            if (!((rb[r] >> lane) & 1u)) {
+                const int64_t q = sb + r * 32 + lane - before - __popc(rb[r] & ltm);
+                if (q >= 0 && q < a.n) { __stcs(a.xo + q, px[r]); __stcs(a.yo + q, py[r]); __stcs(a.zo + q, pz[r]); }
+                __stcs(a.new_index + i, (int32_t)q);
+            } else {
+                __stcs(a.new_index + i, -1);
+            }
+        }
+        before += __popc(rb[r]);
+    }
+}
+
+// Union of the slab masks of a segment's m member records (warp-wide).
+__device__ __forceinline__ uint64_t segment_union(const MemberRec* rec, int m, int lane)
+{
+    uint64_t u = 0;
+    for (int e = lane; e < m; e += 32) u |= __ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].mask));
+    const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)u);
+    const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(u >> 32));
+    return ((uint64_t)hi << 32) | lo;
+}
+
+// The matter step in one cooperative launch.  CTA k owns a contiguous range
+// of 128-atom segments; its warps take every eighth segment of it.
+//   Phase 1 (positions from HBM, kept in L2): per segment the bounding box of
+//     its atoms, the loops whose slab can reach it, and for those (rare)
+//     segments the FP32 pre-test and the exact FP64 tests of the candidate
+//     (atom, loop) pairs queued per warp and spread over its lanes; the
+//     segment's member records are written in atom order into a block taken
+//     from a global counter, and per segment its removed and member counts;
+//     per CTA the counts of every category.
+//   Grid barrier; CTA c scans category c over the CTAs; grid barrier.
+//   Phase 2 (positions again, from L2): per chunk of 32 segments, the warps
+//     copy the survivors of their segments to their final ranks (a segment
+//     without removed atoms is a shifted copy), and when the chunk holds slab
+//     members the CTA writes their slab entries and interstitial copies in
+//     atom order at loop base + CTA prefix + chunk prefix + rank (loop order,
+//     then slab order: Code/prismatic.cpp:61-72, Code/main.cpp:651-654,676-679).
+// No look-back and no second kernel: the only waits are the two barriers.
+// The outputs must not overlap the positions.
+__global__ void __launch_bounds__(kMatterThreads, 4) matter_kernel(const MatterArgs a)
 {
     extern __shared__ __align__(16) unsigned char dyn[];
-    uint64_t* smask = reinterpret_cast<uint64_t*>(dyn);
-    uint64_t* ssides = smask + kMatterTile;
     __shared__ SlabHead sh[kMaxSlabLoops];
-    __shared__ int cnt_s[kMatterWarps * kMatterAtoms];         // survivors per (warp, round), then prefixes
-    __shared__ int cnt_m[kMatterWarps * kMatterAtoms];         // members per (warp, round), then prefixes
-    __shared__ int cnt_c[2 * kMaxSlabLoops];                   // slab and kept-copy counts per loop
-    __shared__ int64_t excl[kMaxCats];
-    __shared__ int aggv[2];
-    __shared__ int s_k;
+    __shared__ int cnt_c[kMaxCats];                             // this CTA's counts per category
     __shared__ int wq[kMatterWarps][kWarpQueue];                // per warp: (slot, loop) pairs to test
     __shared__ int wq_n[kMatterWarps];
+    __shared__ int64_t run[kSegRow];                            // phase 2: next slab entry / copy per loop
+    __shared__ int ctot[kSegRow];                               // phase 2: a chunk's counts per loop category
+    __shared__ int64_t scan_w[kMatterWarps];
     __shared__ unsigned long long vac_s;
-    __shared__ int tile_s;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nl = a.nl, C = a.C;
-    if (tid == 0) { tile_s = (int)atomicAdd(a.ticket, 1u); vac_s = 0ull; }
+    const int nl = a.nl, C = a.C, G = a.G;
+    const int64_t k = blockIdx.x;
+    const int64_t seg_lo = k * a.S / G, seg_hi = (k + 1) * a.S / G;
+    int* err = reinterpret_cast<int*>(a.ctl + 3);
+    const unsigned ltm = (1u << lane) - 1u;
     {
         const int words = nl * (int)(sizeof(SlabHead) / 8);
         const uint64_t* src = reinterpret_cast<const uint64_t*>(a.heads);
         uint64_t* dst = reinterpret_cast<uint64_t*>(sh);
         for (int i = tid; i < words; i += kMatterThreads) dst[i] = src[i];
-        for (int i = tid; i < 2 * nl; i += kMatterThreads) cnt_c[i] = 0;
+        for (int i = tid; i < C; i += kMatterThreads) cnt_c[i] = 0;
+        if (tid == 0) vac_s = 0ull;
     }
     __syncthreads();
     if (tid < nl && sh[tid].type == DISCO_MATTER_VACANCY) atomicOr(&vac_s, 1ull << tid);
-    const int64_t tile = tile_s;
-    const int64_t wbase = tile * kMatterTile + (int64_t)warp * (32 * kMatterAtoms);   // this warp's atoms
-
-    // the warp's bounding box (its atoms come from HBM here; the later reads
-    // of the same 6 KB hit L1/L2) and the loops whose slab can reach it
-    double lo[3] = { 1e300, 1e300, 1e300 }, hi[3] = { -1e300, -1e300, -1e300 };
-#pragma unroll
-    for (int r = 0; r < kMatterAtoms; ++r) {
-        const int64_t i = wbase + r * 32 + lane;
-        if (i < a.n) {
-            const double px = a.x[i], py = a.y[i], pz = a.z[i];
-            lo[0] = fmin(lo[0], px); hi[0] = fmax(hi[0], px);
-            lo[1] = fmin(lo[1], py); hi[1] = fmax(hi[1], py);
-            lo[2] = fmin(lo[2], pz); hi[2] = fmax(hi[2], pz);
-        }
-    }
-    uint64_t wmask = 0;
-    if (nl > 0) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            for (int o = 16; o > 0; o >>= 1) {
-                lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
-                hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
-            }
-        for (int half = 0; half < 2; ++half) {
-            const int l = lane + 32 * half;
-            bool reach = false;
-            if (l < nl && lo[0] <= hi[0]) {
-                const SlabHead& S = sh[l];
-                const double gx = periodic_gap(lo[0], hi[0], S.cx, a.Lx);
-                const double gy = periodic_gap(lo[1], hi[1], S.cy, a.Ly);
-                const double gz = periodic_gap(lo[2], hi[2], S.cz, a.Lz);
-                reach = !(gx * gx + gy * gy + gz * gz > S.bound * S.bound);
-            }
-            wmask |= (uint64_t)__ballot_sync(0xffffffffu, reach) << (32 * half);
-        }
-    }
-    __syncthreads();                                        // vac_s
+    __syncthreads();
     const uint64_t vac = vac_s;
 
-    // every atom's mask, once: the FP32 pre-test per atom, its candidate
-    // (atom, loop) pairs queued per warp, the exact FP64 tests of the queue
-    // spread over the warp's lanes (one latency chain per 32 pairs rather than
-    // one per round and loop), then the counts per (warp, round) and per loop
-    const int wt = warp * (32 * kMatterAtoms);              // the warp's first atom in the tile
-    if (lane == 0) wq_n[warp] = 0;
-    __syncwarp();
-#pragma unroll 1
-    for (int r = 0; r < kMatterAtoms; ++r) {
-        const int64_t i = wbase + r * 32 + lane;
-        uint64_t cand = 0;
-        if (i < a.n && wmask) cand = pretest(sh, wmask, a.x[i], a.y[i], a.z[i], a);
-        smask[wt + r * 32 + lane] = 0;
-        ssides[wt + r * 32 + lane] = 0;
-        for (uint64_t c = cand; c; c &= c - 1) {
-            const int l = __ffsll((long long)c) - 1;
-            const int q = atomicAdd(&wq_n[warp], 1);
-            if (q < kWarpQueue) {
-                wq[warp][q] = (r * 32 + lane) | (l << 16);
-            } else {                                         // a full queue: test here
-                bool ps = false;
-                if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy, a.idLz, ps)) {
-                    smask[wt + r * 32 + lane] |= 1ull << l;
-                    if (ps) ssides[wt + r * 32 + lane] |= 1ull << l;
+    // ---- phase 1: masks and counts --------------------------------------------------
+    {
+        const uint64_t keep = l2_policy_keep();
+        uint64_t* smask = reinterpret_cast<uint64_t*>(dyn) + warp * (2 * kSegAtoms);
+        uint64_t* ssides = smask + kSegAtoms;
+        int w_removed = 0, w_members = 0;
+        for (int64_t s = seg_lo + warp; s < seg_hi; s += kMatterWarps) {
+            const int64_t i0 = s * kSegAtoms;
+            double lo[3] = { 1e300, 1e300, 1e300 }, hi[3] = { -1e300, -1e300, -1e300 };
+            {
+                double px[kSegRounds], py[kSegRounds], pz[kSegRounds];
+#pragma unroll
+                for (int r = 0; r < kSegRounds; ++r) {
+                    const int64_t i = i0 + r * 32 + lane;
+                    px[r] = py[r] = pz[r] = 0.0;
+                    if (i < a.n) { px[r] = ld_hint(a.x + i, keep); py[r] = ld_hint(a.y + i, keep); pz[r] = ld_hint(a.z + i, keep); }
+                }
+#pragma unroll
+                for (int r = 0; r < kSegRounds; ++r)
+                    if (i0 + r * 32 + lane < a.n) {
+                        lo[0] = fmin(lo[0], px[r]); hi[0] = fmax(hi[0], px[r]);
+                        lo[1] = fmin(lo[1], py[r]); hi[1] = fmax(hi[1], py[r]);
+                        lo[2] = fmin(lo[2], pz[r]); hi[2] = fmax(hi[2], pz[r]);
+                    }
+            }
+            uint64_t wmask = 0;
+            if (nl > 0) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    for (int o = 16; o > 0; o >>= 1) {
+                        lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                        hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+                    }
+                for (int half = 0; half * 32 < nl; ++half) {
+                    const int l = lane + 32 * half;
+                    bool reach = false;
+                    if (l < nl) {
+                        const SlabHead& S = sh[l];
+                        const double gx = periodic_gap(lo[0], hi[0], S.cx, a.Lx);
+                        const double gy = periodic_gap(lo[1], hi[1], S.cy, a.Ly);
+                        const double gz = periodic_gap(lo[2], hi[2], S.cz, a.Lz);
+                        reach = !(gx * gx + gy * gy + gz * gz > S.bound * S.bound);
+                    }
+                    wmask |= (uint64_t)__ballot_sync(0xffffffffu, reach) << (32 * half);
                 }
             }
-        }
-    }
-    __syncwarp();
-    {
-        const int nq = min(wq_n[warp], kWarpQueue);
-        for (int q = lane; q < nq; q += 32) {
-            const int slot = wq[warp][q] & 0xffff, l = wq[warp][q] >> 16;
-            const int64_t i = wbase + slot;
-            bool ps = false;
-            if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy, a.idLz, ps)) {
-                atomicOr(reinterpret_cast<unsigned long long*>(&smask[wt + slot]), 1ull << l);
-                if (ps) atomicOr(reinterpret_cast<unsigned long long*>(&ssides[wt + slot]), 1ull << l);
-            }
-        }
-    }
-    __syncwarp();
+            int rc = 0, mc = 0, off = 0;
+            if (wmask) {
+                // the pre-test per atom, its candidate (atom, loop) pairs queued,
+                // the exact tests of the queue spread over the lanes
+#pragma unroll
+                for (int r = 0; r < kSegRounds; ++r) { smask[r * 32 + lane] = 0; ssides[r * 32 + lane] = 0; }
+                if (lane == 0) wq_n[warp] = 0;
+                __syncwarp();
 #pragma unroll 1
-    for (int r = 0; r < kMatterAtoms; ++r) {
-        const int64_t i = wbase + r * 32 + lane;
-        const uint64_t mask = smask[wt + r * 32 + lane];
-        const bool removed = (mask & vac) != 0;
-        const unsigned bs = __ballot_sync(0xffffffffu, i < a.n && !removed);
-        const unsigned bm = __ballot_sync(0xffffffffu, mask != 0);
-        if (lane == 0) { cnt_s[warp * kMatterAtoms + r] = __popc(bs); cnt_m[warp * kMatterAtoms + r] = __popc(bm); }
-        for (uint64_t m = mask; m; m &= m - 1) {             // members are rare
-            const int l = __ffsll((long long)m) - 1;
-            atomicAdd(&cnt_c[l], 1);
-            if (sh[l].type == DISCO_MATTER_INTERSTITIAL && !removed) atomicAdd(&cnt_c[nl + l], 1);
+                for (int r = 0; r < kSegRounds; ++r) {
+                    const int64_t i = i0 + r * 32 + lane;
+                    uint64_t cand = 0;
+                    if (i < a.n) cand = pretest(sh, wmask, a.x[i], a.y[i], a.z[i], a);
+                    for (uint64_t c = cand; c; c &= c - 1) {
+                        const int l = __ffsll((long long)c) - 1;
+                        const int q = atomicAdd(&wq_n[warp], 1);
+                        if (q < kWarpQueue) {
+                            wq[warp][q] = (r * 32 + lane) | (l << 16);
+                        } else {                                 // a full queue: test here
+                            bool ps = false;
+                            if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy,
+                                            a.idLz, ps)) {
+                                atomicOr(reinterpret_cast<unsigned long long*>(&smask[r * 32 + lane]), 1ull << l);
+                                if (ps) atomicOr(reinterpret_cast<unsigned long long*>(&ssides[r * 32 + lane]), 1ull << l);
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                const int nq = min(wq_n[warp], kWarpQueue);
+                for (int q = lane; q < nq; q += 32) {
+                    const int slot = wq[warp][q] & 0xffff, l = wq[warp][q] >> 16;
+                    const int64_t i = i0 + slot;
+                    bool ps = false;
+                    if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy, a.idLz, ps)) {
+                        atomicOr(reinterpret_cast<unsigned long long*>(&smask[slot]), 1ull << l);
+                        if (ps) atomicOr(reinterpret_cast<unsigned long long*>(&ssides[slot]), 1ull << l);
+                    }
+                }
+                __syncwarp();
+                // counts, then the member records in atom order
+                unsigned bm[kSegRounds];
+#pragma unroll
+                for (int r = 0; r < kSegRounds; ++r) {
+                    const uint64_t mask = smask[r * 32 + lane];
+                    const bool removed = (mask & vac) != 0;
+                    bm[r] = __ballot_sync(0xffffffffu, mask != 0);
+                    rc += __popc(__ballot_sync(0xffffffffu, removed));
+                    mc += __popc(bm[r]);
+                    for (uint64_t u = mask; u; u &= u - 1) {     // members are rare
+                        const int l = __ffsll((long long)u) - 1;
+                        atomicAdd(&cnt_c[2 + l], 1);
+                        if (sh[l].type == DISCO_MATTER_INTERSTITIAL && !removed) atomicAdd(&cnt_c[2 + nl + l], 1);
+                    }
+                }
+                if (lane == 0) off = (int)atomicAdd(a.ctl + 2, (unsigned)mc);
+                off = __shfl_sync(0xffffffffu, off, 0);
+                int e = off;
+#pragma unroll
+                for (int r = 0; r < kSegRounds; ++r) {
+                    const uint64_t mask = smask[r * 32 + lane];
+                    if (mask) {
+                        const int64_t q = (int64_t)e + __popc(bm[r] & ltm);
+                        if (q < a.member_cap) {
+                            MemberRec rec;
+                            rec.atom = (int32_t)(i0 + r * 32 + lane);
+                            rec.removed = (mask & vac) != 0;
+                            rec.mask = mask;
+                            rec.sides = ssides[r * 32 + lane];
+                            a.members[q] = rec;
+                        }
+                    }
+                    e += __popc(bm[r]);
+                }
+            }
+            if (lane == 0) { a.seg_removed[s] = rc; a.seg_members[s] = mc; a.seg_off[s] = off; }
+            w_removed += rc;
+            w_members += mc;
         }
+        if (lane == 0) { atomicAdd(&cnt_c[0], w_removed); atomicAdd(&cnt_c[1], w_members); }
     }
     __syncthreads();
+    {
+        const int64_t e_hi = seg_hi * kSegAtoms < a.n ? seg_hi * kSegAtoms : a.n;
+        const int64_t atoms_k = seg_hi > seg_lo ? e_hi - seg_lo * kSegAtoms : 0;
+        for (int c = tid; c < C; c += kMatterThreads)
+            a.cta_tot[k * C + c] = c == 0 ? (int32_t)(atoms_k - cnt_c[0]) : cnt_c[c];
+    }
+    grid_sync(a.ctl, (unsigned)G, err);
 
-    // warps 0 and 1: prefixes over (warp, round) in atom order and the tile's
-    // survivor and member counts
-    if (warp < 2) {
-        int* cnt = warp == 0 ? cnt_s : cnt_m;
-        constexpr int kPer = kMatterAtoms * kMatterWarps / 32;  // 2 entries per lane
-        int v[kPer], tot = 0;
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) { v[j] = cnt[lane * kPer + j]; tot += v[j]; }
-        int incl = tot;
+    // ---- scan: CTA c takes category c, exclusive prefixes over the CTAs --------------
+    for (int c = blockIdx.x; c < C; c += G) {
+        const int per = (G + kMatterThreads - 1) / kMatterThreads;
+        const int k0 = tid * per;
+        int64_t sum = 0;
+        for (int q = 0; q < per; ++q)
+            if (k0 + q < G) sum += __ldcg(a.cta_tot + (int64_t)(k0 + q) * C + c);
+        int64_t incl = sum;
         for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            const int64_t y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        int run = incl - tot;
-#pragma unroll
-        for (int j = 0; j < kPer; ++j) { cnt[lane * kPer + j] = run; run += v[j]; }
-        if (lane == 31) aggv[warp] = incl;
-    }
-    __syncthreads();
-
-    // decoupled look-back: publish the tile's counts, then one warp scans the
-    // flags of the 32 preceding tiles at a time for the nearest published
-    // inclusive prefix (every tile between must have published its counts),
-    // and every category's thread sums that window's values
-    const int32_t my_agg = tid < C ? (tid < 2 ? aggv[tid] : cnt_c[tid - 2]) : 0;
-    if (tid < C) {
-        a.agg[tile * C + tid] = my_agg;
-        if (tile == 0) a.inc[tid] = my_agg;
-        __threadfence();
-    }
-    __syncthreads();
-    if (tid == 0) st_release(a.flags + tile, tile == 0 ? kFlagInc : kFlagAgg);
-    int64_t pre = 0;
-    if (tile > 0) {
-        int64_t jhi = tile - 1;                                 // top of the window
-        while (true) {
-            if (warp == 0) {
-                unsigned long long t0 = 0;
-                int k;
-                while (true) {
-                    const int64_t j = jhi - lane;
-                    const int f = j >= 0 ? ld_acquire(a.flags + j) : kFlagAgg;
-                    const unsigned bi = __ballot_sync(0xffffffffu, f == kFlagInc);
-                    const unsigned br = __ballot_sync(0xffffffffu, f >= kFlagAgg);
-                    k = bi ? __ffs(bi) - 1 : 32;                 // nearest inclusive prefix
-                    const unsigned need = k == 32 ? 0xffffffffu : ((1u << k) - 1u);
-                    if ((br & need) == need) break;
-                    if (t0 == 0) t0 = global_ns();
-                    else if (global_ns() - t0 > kWaitLimitNs) {
-                        if (lane == 0) report(a.err, DISCO_ETIMEOUT);
-                        k = -1;
-                        break;
-                    }
-                }
-                if (lane == 0) s_k = k;
-            }
-            __syncthreads();
-            const int k = s_k;
-            if (k < 0) break;                                   // gave up: publish anyway
-            if (tid < C) {
-                for (int q = 0; q < k; ++q) pre += __ldcg(a.agg + (jhi - q) * C + tid);
-                if (k < 32) pre += __ldcg(a.inc + (jhi - k) * C + tid);
-            }
-            if (k < 32) break;
-            jhi -= 32;
-            __syncthreads();                                    // s_k is rewritten
-        }
-    }
-    if (tid < C) {
-        if (tile > 0) a.inc[tile * C + tid] = (int32_t)(pre + my_agg);
-        excl[tid] = pre;
-        __threadfence();
-    }
-    __syncthreads();
-    if (tid == 0 && tile > 0) st_release(a.flags + tile, kFlagInc);
-
-    // survivors at their final ranks, the new-index map, member records
-    const unsigned ltm = (1u << lane) - 1u;
-#pragma unroll 2
-    for (int r = 0; r < kMatterAtoms; ++r) {
-        const int64_t i = wbase + r * 32 + lane;
-        const bool valid = i < a.n;
-        const uint64_t mask = smask[wt + r * 32 + lane];
-        const bool surv = valid && !(mask & vac);
-        const unsigned bs = __ballot_sync(0xffffffffu, surv);
-        const unsigned bm = __ballot_sync(0xffffffffu, mask != 0);
-        if (valid) {
-            if (surv) {
-                const int64_t q = excl[0] + cnt_s[warp * kMatterAtoms + r] + __popc(bs & ltm);
-                if (q < a.n) { a.xo[q] = a.x[i]; a.yo[q] = a.y[i]; a.zo[q] = a.z[i]; }
-                a.new_index[i] = (int32_t)q;
-            } else {
-                a.new_index[i] = -1;
-            }
-        }
-        if (mask) {
-            const int64_t q = excl[1] + cnt_m[warp * kMatterAtoms + r] + __popc(bm & ltm);
-            if (q < a.member_cap) {
-                MemberRec m;
-                m.atom = (int32_t)i;
-                m.removed = (mask & vac) != 0;
-                m.mask = mask;
-                m.sides = ssides[wt + r * 32 + lane];
-                a.members[q] = m;
-            }
-        }
-    }
-}
-
-// The slab entries and the interstitial copies, from the member records of
-// each tile (tiles spread over the CTAs, after the pass): entry of loop l
-// at loop base + the tile's exclusive count of loop l + its rank among the
-// tile's members in l (ascending atom order, Code/prismatic.cpp:61-72); a copy
-// of an interstitial loop's entry whose atom survives at copy base + the tile's
-// exclusive kept count + its rank (loop order, then slab order; sources
-// renumbered, Code/main.cpp:651-654,676-679).  CTA 0 also writes the totals.
-__global__ void __launch_bounds__(256) matter_tail_kernel(const MatterArgs a, int64_t ntiles)
-{
-    __shared__ int64_t tot[kMaxCats];
-    __shared__ int64_t lbase[kMaxSlabLoops], cbase[kMaxSlabLoops];
-    __shared__ int run[2 * kMaxSlabLoops];
-    __shared__ int wc[8][2];
-    __shared__ unsigned long long umask;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nl = a.nl, C = a.C;
-    // totals = the last tile's inclusive counts; loop and copy bases
-    for (int c = tid; c < C; c += 256) tot[c] = a.inc[(ntiles - 1) * C + c];
-    __syncthreads();
-    if (tid == 0) {
-        int64_t sb = 0, cb = 0;
-        for (int l = 0; l < nl; ++l) {
-            lbase[l] = sb; sb += tot[2 + l];
-            cbase[l] = cb; cb += tot[2 + nl + l];
-        }
-        if (blockIdx.x == 0) {
-            for (int c = 0; c < C; ++c) a.totals[c] = tot[c];
-            a.totals[C] = *a.err;                              // the pass's error word
-            *a.err = 0;                                        // ticket and error word cleared
-            *a.ticket = 0;                                     // for the next call
-        }
-    }
-    // this CTA's tiles (grid-stride): each tile's flag cleared for the next
-    // call (the pass is over), its member records turned into entries
-    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        if (tid == 0) a.flags[t] = 0;
-        const int64_t mend = a.inc[t * C + 1];                           // this tile's member records
-        const int64_t m0 = mend - a.agg[t * C + 1];
-        if (mend == m0) continue;
-        __syncthreads();                                    // run / umask of the previous tile
-        if (tid == 0) umask = 0ull;
-        for (int i = tid; i < 2 * nl; i += 256) run[i] = 0;
+        if (lane == 31) scan_w[warp] = incl;
         __syncthreads();
-        for (int64_t e0 = m0; e0 < mend; e0 += 256) {
-            const int64_t e = e0 + tid;
-            MemberRec m;
-            m.atom = 0; m.removed = 1; m.mask = 0; m.sides = 0;
-            if (e < mend && e < a.member_cap) m = a.members[e];
-            if (m.mask) atomicOr(&umask, m.mask);
-            __syncthreads();
-            const uint64_t um = umask;
-            for (uint64_t u = um; u; u &= u - 1) {
-                const int l = __ffsll((long long)u) - 1;
-                const bool in = (m.mask >> l) & 1ull;
-                const bool keep = in && !m.removed && a.heads[l].type == DISCO_MATTER_INTERSTITIAL;
-                const unsigned bi = __ballot_sync(0xffffffffu, in);
-                const unsigned bk = __ballot_sync(0xffffffffu, keep);
-                if (lane == 0) { wc[warp][0] = __popc(bi); wc[warp][1] = __popc(bk); }
-                __syncthreads();
-                int pi = run[l], pk = run[nl + l];
-                for (int w = 0; w < warp; ++w) { pi += wc[w][0]; pk += wc[w][1]; }
-                const unsigned ltm = (1u << lane) - 1u;
-                if (in) {
-                    const int64_t q = lbase[l] + (a.inc[t * C + 2 + l] - a.agg[t * C + 2 + l]) + pi +
-                                      __popc(bi & ltm);
-                    if (q < a.slab_cap) {
-                        a.slab_atoms[q] = m.atom;
-                        a.slab_side[q] = ((m.sides >> l) & 1ull) ? 1 : -1;
-                    }
-                }
-                if (keep) {
-                    const int64_t q = cbase[l] + (a.inc[t * C + 2 + nl + l] - a.agg[t * C + 2 + nl + l]) + pk +
-                                      __popc(bk & ltm);
-                    if (q < a.copy_cap) {
-                        const disco_slab_loop& g = a.loops[l].L;
-                        const double* sh = ((m.sides >> l) & 1ull) ? g.shift_pos : g.shift_neg;
-                        disco_copy cp;
-                        cp.atom = a.new_index[m.atom];
-                        cp.reserved = 0;
-                        cp.shift[0] = sh[0]; cp.shift[1] = sh[1]; cp.shift[2] = sh[2];
-                        a.copies[q] = cp;
-                    }
-                }
-                __syncthreads();
-                if (tid == 0) {
-                    for (int w = 0; w < 8; ++w) { run[l] += wc[w][0]; run[nl + l] += wc[w][1]; }
-                }
-                __syncthreads();
+        int64_t runv = incl - sum, total = 0;
+        for (int w = 0; w < kMatterWarps; ++w) {
+            if (w < warp) runv += scan_w[w];
+            total += scan_w[w];
+        }
+        for (int q = 0; q < per; ++q)
+            if (k0 + q < G) {
+                const int32_t v = __ldcg(a.cta_tot + (int64_t)(k0 + q) * C + c);
+                a.cta_pre[(int64_t)(k0 + q) * C + c] = (int32_t)runv;
+                runv += v;
             }
-            if (tid == 0) umask = 0ull;
-            __syncthreads();
+        if (tid == 0) a.totals[c] = total;
+        __syncthreads();                                        // scan_w is rewritten
+    }
+    grid_sync(a.ctl, 2u * (unsigned)G, err);
+
+    // ---- phase 2: survivors, slab entries, copies -------------------------------------
+    if (warp == 0) {
+        // loop bases (exclusive scans over the loops' totals) plus this CTA's prefix
+        int64_t sb = 0, cb = 0;
+        for (int l0 = 0; l0 < nl; l0 += 32) {
+            const int l = l0 + lane;
+            const int64_t ts = l < nl ? __ldcg(a.totals + 2 + l) : 0;
+            const int64_t tc = l < nl ? __ldcg(a.totals + 2 + nl + l) : 0;
+            int64_t is = ts, ic = tc;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t ys = __shfl_up_sync(0xffffffffu, is, o);
+                const int64_t yc = __shfl_up_sync(0xffffffffu, ic, o);
+                if (lane >= o) { is += ys; ic += yc; }
+            }
+            if (l < nl) {
+                run[l] = sb + is - ts + __ldcg(a.cta_pre + k * C + 2 + l);
+                run[nl + l] = cb + ic - tc + __ldcg(a.cta_pre + k * C + 2 + nl + l);
+            }
+            sb += __shfl_sync(0xffffffffu, is, 31);
+            cb += __shfl_sync(0xffffffffu, ic, 31);
+        }
+    }
+    __syncthreads();
+    {
+        const uint64_t last = l2_policy_last_use();
+        const int64_t surv_k = __ldcg(a.cta_pre + k * C);
+        int* segrel = reinterpret_cast<int*>(dyn);              // [kChunkSegs][kSegRow]
+        int64_t rem_run = 0;                                    // removed atoms of the CTA's earlier chunks
+        for (int64_t c0 = seg_lo; c0 < seg_hi; c0 += kChunkSegs) {
+            const int cn = (int)(seg_hi - c0 < kChunkSegs ? seg_hi - c0 : kChunkSegs);
+            const int v_rem = lane < cn ? __ldcg(a.seg_removed + c0 + lane) : 0;
+            const int v_mem = lane < cn ? __ldcg(a.seg_members + c0 + lane) : 0;
+            const int v_off = lane < cn ? __ldcg(a.seg_off + c0 + lane) : 0;
+            int incl = v_rem;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int ex_rem = incl - v_rem;
+            const int chunk_rem = __shfl_sync(0xffffffffu, incl, 31);
+            const bool any_mem = __ballot_sync(0xffffffffu, v_mem > 0) != 0;   // the same in every warp
+            const int64_t base = surv_k + (c0 - seg_lo) * kSegAtoms - rem_run; // survivors before the chunk
+#pragma unroll 1
+            for (int rr = 0; rr < kChunkSegs / kMatterWarps; ++rr) {
+                const int j = rr * kMatterWarps + warp;
+                if (j >= cn) break;
+                const int64_t sbj = base + (int64_t)j * kSegAtoms - __shfl_sync(0xffffffffu, ex_rem, j);
+                copy_segment(a, c0 + j, sbj, __shfl_sync(0xffffffffu, v_rem, j), __shfl_sync(0xffffffffu, v_mem, j),
+                             __shfl_sync(0xffffffffu, v_off, j), last, lane);
+            }
+            if (any_mem) {
+                // per-loop slab and kept-copy counts of each segment of the chunk
+#pragma unroll 1
+                for (int rr = 0; rr < kChunkSegs / kMatterWarps; ++rr) {
+                    const int j = rr * kMatterWarps + warp;
+                    for (int c = lane; c < 2 * nl; c += 32) segrel[j * kSegRow + c] = 0;
+                    __syncwarp();
+                    const int m = __shfl_sync(0xffffffffu, v_mem, j), off = __shfl_sync(0xffffffffu, v_off, j);
+                    if (j < cn && m > 0 && (int64_t)off + m <= a.member_cap) {
+                        const MemberRec* rec = a.members + off;
+                        for (uint64_t u = segment_union(rec, m, lane); u; u &= u - 1) {
+                            const int l = __ffsll((long long)u) - 1;
+                            const bool inter = sh[l].type == DISCO_MATTER_INTERSTITIAL;
+                            int cin = 0, ck = 0;
+                            for (int e0 = 0; e0 < m; e0 += 32) {
+                                const int e = e0 + lane;
+                                bool in = false, kp = false;
+                                if (e < m) {
+                                    in = (__ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].mask)) >> l) & 1ull;
+                                    kp = in && inter && !__ldcg(&rec[e].removed);
+                                }
+                                cin += __popc(__ballot_sync(0xffffffffu, in));
+                                ck += __popc(__ballot_sync(0xffffffffu, kp));
+                            }
+                            if (lane == 0) { segrel[j * kSegRow + l] = cin; segrel[j * kSegRow + nl + l] = ck; }
+                        }
+                    }
+                }
+                __syncthreads();
+                // exclusive prefixes over the chunk's segments, per category
+                for (int c = warp; c < 2 * nl; c += kMatterWarps) {
+                    const int v = segrel[lane * kSegRow + c];
+                    int p = v;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, p, o);
+                        if (lane >= o) p += y;
+                    }
+                    segrel[lane * kSegRow + c] = p - v;
+                    if (lane == 31) ctot[c] = p;
+                }
+                __syncthreads();
+                // slab entries and copies, ascending atom order within each loop
+#pragma unroll 1
+                for (int rr = 0; rr < kChunkSegs / kMatterWarps; ++rr) {
+                    const int j = rr * kMatterWarps + warp;
+                    const int m = __shfl_sync(0xffffffffu, v_mem, j), off = __shfl_sync(0xffffffffu, v_off, j);
+                    const int exr = __shfl_sync(0xffffffffu, ex_rem, j);
+                    if (j < cn && m > 0 && (int64_t)off + m <= a.member_cap) {
+                        const MemberRec* rec = a.members + off;
+                        const int64_t i0 = (c0 + j) * kSegAtoms;
+                        const int64_t sbj = base + (int64_t)j * kSegAtoms - exr;
+                        for (uint64_t u = segment_union(rec, m, lane); u; u &= u - 1) {
+                            const int l = __ffsll((long long)u) - 1;
+                            const bool inter = sh[l].type == DISCO_MATTER_INTERSTITIAL;
+                            int64_t qs = run[l] + segrel[j * kSegRow + l];
+                            int64_t qc = run[nl + l] + segrel[j * kSegRow + nl + l];
+                            int rem_before = 0;
+                            for (int e0 = 0; e0 < m; e0 += 32) {
+                                const int e = e0 + lane;
+                                MemberRec r;
+                                r.atom = 0; r.removed = 0; r.mask = 0; r.sides = 0;
+                                if (e < m) {
+                                    r.atom = __ldcg(&rec[e].atom);
+                                    r.removed = __ldcg(&rec[e].removed);
+                                    r.mask = __ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].mask));
+                                    r.sides = __ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].sides));
+                                }
+                                const bool in = (r.mask >> l) & 1ull;
+                                const bool kp = in && inter && !r.removed;
+                                const unsigned bi = __ballot_sync(0xffffffffu, in);
+                                const unsigned bk = __ballot_sync(0xffffffffu, kp);
+                                const unsigned br = __ballot_sync(0xffffffffu, e < m && r.removed);
+                                const bool pos = (r.sides >> l) & 1ull;
+                                if (in) {
+                                    const int64_t q = qs + __popc(bi & ltm);
+                                    if (q >= 0 && q < a.slab_cap) { a.slab_atoms[q] = r.atom; a.slab_side[q] = pos ? 1 : -1; }
+                                }
+                                if (kp) {
+                                    const int64_t q = qc + __popc(bk & ltm);
+                                    if (q >= 0 && q < a.copy_cap) {
+                                        const disco_slab_loop& g = a.loops[l].L;
+                                        const double* shf = pos ? g.shift_pos : g.shift_neg;
+                                        disco_copy cp;
+                                        cp.atom = (int32_t)(sbj + (r.atom - i0) - (rem_before + __popc(br & ltm)));
+                                        cp.reserved = 0;
+                                        cp.shift[0] = shf[0]; cp.shift[1] = shf[1]; cp.shift[2] = shf[2];
+                                        a.copies[q] = cp;
+                                    }
+                                }
+                                qs += __popc(bi);
+                                qc += __popc(bk);
+                                rem_before += __popc(br);
+                            }
+                        }
+                    }
+                }
+                __syncthreads();                                // segrel and run are rewritten
+                for (int c = tid; c < 2 * nl; c += kMatterThreads) run[c] += ctot[c];
+            }
+            rem_run += chunk_rem;
+        }
+    }
+
+    // the last CTA to leave hands the error word over and clears the control words
+    if (tid == 0) {
+        __threadfence();
+        const unsigned done = atomicAdd(a.ctl + 1, 1u);
+        if (done == (unsigned)G - 1u) {
+            a.totals[C] = atomicExch(err, 0);
+            atomicExch(a.ctl + 0, 0u);
+            atomicExch(a.ctl + 2, 0u);
+            atomicExch(a.ctl + 1, 0u);
         }
     }
 }
@@ -825,23 +966,55 @@ int stage_loops(const disco_slab_loop* loops, int nloops, const double box[3], d
     return DISCO_OK;
 }
 
-// Bytes of the look-back flags (ticket and error word first), cleared per call.
-size_t status_bytes(int64_t ntiles) { return 16 + (size_t)ntiles * sizeof(int); }
+// Bytes of the control words (barrier arrivals, exits, member records taken,
+// error word); the last CTA of every completed call leaves them at zero.
+constexpr size_t kCtlBytes = 16;
+
+// CTAs of the cooperative launch on the current device: resident CTAs per SM
+// times the SM count, at most kMaxGrid (cached per device; no allocation).
+int matter_grid_max(int& out)
+{
+    static std::mutex mu;
+    static int cached[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cfail(e, "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= 0 && dev < 64 && cached[dev] > 0) { out = cached[dev]; return DISCO_OK; }
+    int coop = 0, sms = 0, per_sm = 0;
+    e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, disco::matter_kernel, disco::kMatterThreads,
+                                                          disco::kMatterSmem);
+    if (e != cudaSuccess) return cfail(e, "matter step occupancy");
+    if (!coop || per_sm < 1 || sms < 1) return efail(DISCO_ENODEV, "the device takes no cooperative launch of the matter step");
+    out = std::min(per_sm * sms, disco::kMaxGrid);
+    if (dev >= 0 && dev < 64) cached[dev] = out;
+    return DISCO_OK;
+}
+
+// Segments and CTAs of a call on n atoms.
+void matter_shape(int64_t n, int grid_max, int64_t& S, int& G)
+{
+    S = (n + disco::kSegAtoms - 1) / disco::kSegAtoms;
+    const int64_t want = (S + disco::kMatterWarps - 1) / disco::kMatterWarps;   // a segment per warp at least
+    G = (int)std::max<int64_t>(1, std::min<int64_t>(grid_max, want));
+}
 
 struct MatterScratch {
     unsigned char* loops;        // heads then records (sizeof(LoopStage))
-    unsigned char* status;       // status_bytes(ntiles)
-    int32_t* agg;                // ntiles * C
-    int32_t* inc;                // ntiles * C
+    unsigned int* ctl;           // kCtlBytes
+    int32_t* seg;                // 3 S: removed, members, first record per segment
+    int32_t* cta;                // 2 G C: counts and prefixes per CTA
     disco::MemberRec* members;
     int64_t member_cap;
-    int64_t* totals;             // C + 1 (the last: the kernels' error word)
+    int64_t* totals;             // C + 1 (the last: the kernel's error word)
 };
 
 // Queues the matter step on stream s after stage_loops (no host wait): the
-// look-back words cleared, the single pass, the tail.
-int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int64_t ntiles, cudaStream_t s,
-                 size_t clear_bytes)
+// control words cleared when `clear`, then one cooperative launch of G CTAs.
+int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, int64_t S, int G, cudaStream_t s, bool clear)
 {
     using namespace disco;
     cudaError_t e = cudaSuccess;
@@ -849,33 +1022,31 @@ int matter_queue(disco::MatterArgs& a, const MatterScratch& m, int nl, const int
     a.loops = reinterpret_cast<const SlabLoopDev*>(m.loops + recs_offset(nl));
     a.nl = nl;
     a.C = 2 + 2 * nl;
-    a.flags = reinterpret_cast<int*>(m.status + 16);
-    a.ticket = reinterpret_cast<unsigned int*>(m.status);
-    a.err = reinterpret_cast<int*>(m.status + 4);
-    a.agg = m.agg;
-    a.inc = m.inc;
+    a.G = G;
+    a.S = S;
+    a.seg_removed = m.seg;
+    a.seg_members = m.seg + S;
+    a.seg_off = m.seg + 2 * S;
+    a.cta_tot = m.cta;
+    a.cta_pre = m.cta + (int64_t)G * a.C;
+    a.ctl = m.ctl;
     a.members = m.members;
     a.member_cap = m.member_cap;
     a.totals = m.totals;
-    // the tail of every completed call leaves the flags, ticket and error word
-    // at zero; a caller that cannot rely on that (fresh memory, a call that
-    // failed half-way) clears them here
-    if (clear_bytes) {
-        e = cudaMemsetAsync(m.status, 0, clear_bytes, s);
-        if (e != cudaSuccess) return cfail(e, "look-back reset");
+    // a caller that cannot rely on the previous call's exit (fresh memory, a
+    // call that failed half-way) clears the control words here
+    if (clear) {
+        e = cudaMemsetAsync(m.ctl, 0, kCtlBytes, s);
+        if (e != cudaSuccess) return cfail(e, "matter step control words");
     }
-    if (kMatterSmem > 48 * 1024) {
-        e = cudaFuncSetAttribute(matter_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMatterSmem);
-        if (e != cudaSuccess) return cfail(e, "matter step shared memory");
-    }
-    if (ntiles > 0) {
-        matter_pass_kernel<<<(unsigned)ntiles, kMatterThreads, kMatterSmem, s>>>(a);
-        matter_tail_kernel<<<(unsigned)std::min<int64_t>(ntiles, 512), 256, 0, s>>>(a, ntiles);
+    if (S > 0) {
+        void* params[] = { &a };
+        e = cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(matter_kernel), dim3((unsigned)G),
+                                        dim3(kMatterThreads), params, kMatterSmem, s);
     } else {
         e = cudaMemsetAsync(m.totals, 0, (size_t)(a.C + 1) * sizeof(int64_t), s);
-        if (e != cudaSuccess) return cfail(e, "totals reset");
     }
-    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e != cudaSuccess) return cfail(e, "matter step launch");
     return DISCO_OK;
 }
@@ -951,11 +1122,16 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     }
     if (nl > kMaxSlabLoops) return efail(DISCO_ELIMIT, "more than 64 prismatic loops in one call");
     const int C = 2 + 2 * nl;
-    const int64_t ntiles = (n + kMatterTile - 1) / kMatterTile;
+    int grid_max = 0;
+    int st = matter_grid_max(grid_max);
+    if (st) return st;
+    int64_t S = 0;
+    int G = 1;
+    matter_shape(n, grid_max, S, G);
     const int64_t member_cap = std::max<int64_t>(1, std::min<int64_t>(n, slab_capacity));
     const int64_t scap = std::max<int64_t>(1, slab_capacity), ccap = std::max<int64_t>(1, copy_capacity);
 
-    DevBuf dxyz, dout, didx, dloops, dstat, dagg, dmem, dtot, dslab, dside, dcop;
+    DevBuf dxyz, dout, didx, dloops, dctl, dseg, dcta, dmem, dtot, dslab, dside, dcop;
     const size_t nb = (size_t)n * sizeof(double);
     cudaError_t e = cudaSuccess;
     if (n > 0) {
@@ -964,8 +1140,9 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
         if (e == cudaSuccess) e = cudaMalloc(&didx.p, (size_t)n * sizeof(int32_t));
     }
     if (e == cudaSuccess) e = cudaMalloc(&dloops.p, sizeof(LoopStage));
-    if (e == cudaSuccess) e = cudaMalloc(&dstat.p, status_bytes(ntiles));
-    if (e == cudaSuccess) e = cudaMalloc(&dagg.p, 2 * std::max<int64_t>(1, ntiles * C) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dctl.p, kCtlBytes);
+    if (e == cudaSuccess) e = cudaMalloc(&dseg.p, 3 * std::max<int64_t>(1, S) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&dcta.p, 2 * (size_t)G * C * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&dmem.p, (size_t)member_cap * sizeof(MemberRec));
     if (e == cudaSuccess) e = cudaMalloc(&dtot.p, (size_t)(C + 1) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&dslab.p, (size_t)scap * sizeof(int32_t));
@@ -978,7 +1155,7 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
         if (e == cudaSuccess) e = cudaMemcpy(dxyz.as<double>() + 2 * n, z, nb, cudaMemcpyHostToDevice);
     }
     if (e != cudaSuccess) return cfail(e, "prismatic upload");
-    int st = stage_loops(loops, nloops, box, info, act_index, nl, dloops.as<unsigned char>(), nullptr);
+    st = stage_loops(loops, nloops, box, info, act_index, nl, dloops.as<unsigned char>(), nullptr);
     if (st) return st;
 
     MatterArgs a;
@@ -997,13 +1174,13 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     a.copy_cap = copy_capacity;
     MatterScratch m;
     m.loops = dloops.as<unsigned char>();
-    m.status = dstat.as<unsigned char>();
-    m.agg = dagg.as<int32_t>();
-    m.inc = m.agg + std::max<int64_t>(1, ntiles * C);
+    m.ctl = dctl.as<unsigned int>();
+    m.seg = dseg.as<int32_t>();
+    m.cta = dcta.as<int32_t>();
     m.members = dmem.as<MemberRec>();
     m.member_cap = member_cap;
     m.totals = dtot.as<int64_t>();
-    st = matter_queue(a, m, nl, ntiles, nullptr, status_bytes(ntiles));
+    st = matter_queue(a, m, nl, S, G, nullptr, true);
     if (st) return st;
     int64_t tot[kMaxCats + 1];
     e = cudaMemcpy(tot, m.totals, (size_t)(C + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost);
@@ -1099,23 +1276,23 @@ int disco_b200_finalize_resident(const double* x, const double* y, const double*
 // memory pool, a code that may not synchronise the device the way cudaFree
 // does, a process with a fixed memory budget) cannot let the library call
 // cudaMalloc.  disco_b200_prismatic_noalloc takes device inputs and outputs
-// from the caller and keeps its scratch (loop table, look-back words, per-tile
-// prefixes, member records, totals) in the file-scope array below: 4 MiB
+// from the caller and keeps its scratch (loop table, control words, per-segment
+// and per-CTA counts and prefixes, member records, totals) in the file-scope
+// array below: 4 MiB
 // that every GPU loading this library holds until the process exits.
 
 namespace {
 
 constexpr int64_t kNoAllocMaxAtoms = int64_t(1) << 22;                  // 4 194 304 atoms
-constexpr int64_t kNoAllocMaxTiles = kNoAllocMaxAtoms / disco::kMatterTile;
+constexpr int64_t kNoAllocMaxSegs = kNoAllocMaxAtoms / disco::kSegAtoms;
 constexpr int64_t kNoAllocMaxMembers = int64_t(1) << 16;                // atoms in slabs
 constexpr size_t align256c(size_t v) { return (v + 255) & ~size_t(255); }
 constexpr size_t kNoAllocLoopOff = 0;
-constexpr size_t kNoAllocStatusOff = kNoAllocLoopOff + align256c(sizeof(LoopStage));
-constexpr size_t kNoAllocAggOff = kNoAllocStatusOff + align256c(16 + (size_t)kNoAllocMaxTiles * sizeof(int));
-constexpr size_t kNoAllocIncOff =
-    kNoAllocAggOff + align256c((size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(int32_t));
+constexpr size_t kNoAllocCtlOff = kNoAllocLoopOff + align256c(sizeof(LoopStage));
+constexpr size_t kNoAllocSegOff = kNoAllocCtlOff + align256c(kCtlBytes);
+constexpr size_t kNoAllocCtaOff = kNoAllocSegOff + align256c(3 * (size_t)kNoAllocMaxSegs * sizeof(int32_t));
 constexpr size_t kNoAllocMemberOff =
-    kNoAllocIncOff + align256c((size_t)kNoAllocMaxTiles * disco::kMaxCats * sizeof(int32_t));
+    kNoAllocCtaOff + align256c(2 * (size_t)disco::kMaxGrid * disco::kMaxCats * sizeof(int32_t));
 constexpr size_t kNoAllocTotalsOff =
     kNoAllocMemberOff + align256c((size_t)kNoAllocMaxMembers * sizeof(disco::MemberRec));
 constexpr size_t kNoAllocScratchBytes = 4 * 1024 * 1024;
@@ -1128,7 +1305,7 @@ constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 unsigned char* g_noalloc_addr[kMaxDevices] = {};
 unsigned long long g_noalloc_ctx[kMaxDevices] = {};
-bool g_noalloc_dirty[kMaxDevices] = {};     // the look-back flags may not be zero
+bool g_noalloc_dirty[kMaxDevices] = {};     // the control words may not be zero
 
 using CtxGetCurrentFn = CUresult (*)(CUcontext*);
 using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
@@ -1233,7 +1410,12 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     st = stage_loops(loops, nloops, box, info, act_index, nl, base + kNoAllocLoopOff, s, ctx);
     if (st) return st;
     const int C = 2 + 2 * nl;
-    const int64_t ntiles = (n + kMatterTile - 1) / kMatterTile;
+    int grid_max = 0;
+    st = matter_grid_max(grid_max);
+    if (st) return st;
+    int64_t S = 0;
+    int G = 1;
+    matter_shape(n, grid_max, S, G);
     const int64_t member_cap = std::min<int64_t>(kNoAllocMaxMembers, std::max<int64_t>(0, slab_capacity));
 
     MatterArgs a;
@@ -1252,14 +1434,14 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     a.copy_cap = copy_capacity;
     MatterScratch m;
     m.loops = base + kNoAllocLoopOff;
-    m.status = base + kNoAllocStatusOff;
-    m.agg = reinterpret_cast<int32_t*>(base + kNoAllocAggOff);
-    m.inc = reinterpret_cast<int32_t*>(base + kNoAllocIncOff);
+    m.ctl = reinterpret_cast<unsigned int*>(base + kNoAllocCtlOff);
+    m.seg = reinterpret_cast<int32_t*>(base + kNoAllocSegOff);
+    m.cta = reinterpret_cast<int32_t*>(base + kNoAllocCtaOff);
     m.members = reinterpret_cast<MemberRec*>(base + kNoAllocMemberOff);
     m.member_cap = member_cap;
     m.totals = reinterpret_cast<int64_t*>(base + kNoAllocTotalsOff);
     const bool dirty = noalloc_dirty(dev, true, false);
-    st = matter_queue(a, m, nl, ntiles, s, dirty ? status_bytes(kNoAllocMaxTiles) : 0);
+    st = matter_queue(a, m, nl, S, G, s, dirty);
     if (st) { stage_cache_drop(); noalloc_dirty(dev, false, true); return st; }
     int64_t tot[kMaxCats + 1];
     cudaError_t e = cudaMemcpyAsync(tot, m.totals, (size_t)(C + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s);

@@ -1125,8 +1125,7 @@ def compaction_rate(lib, C, torch, stream):
     positions read once, survivors written, 4 B new index; the slab entries
     and copies add a few hundred KB) against the measured HBM peak.  Timed per
     call with CUDA events around the whole call, which ends with one
-    device-to-host read of the totals (its only host wait); the single-pass
-    kernel alone is timed too."""
+    device-to-host read of the totals (its only host wait)."""
     import ctypes
     from disco_b200 import workloads as W
     w = W.bcc_prismatic(cells=128)
@@ -1163,7 +1162,7 @@ def compaction_rate(lib, C, torch, stream):
     return {"atoms": n, "survivors": int(counts[0]), "slab_atoms": int(counts[1]), "copies": int(counts[2]),
             "ms": 1e3 * t, "atoms_per_s": n / t, "algorithmic_bytes": 52 * n, "achieved_gbs": gbs,
             "peak_gbs": peak, "frac": gbs / peak, "l2": "flushed before each timed call",
-            "timed": "whole call (loop upload, pass, tail, totals read back) with CUDA events",
+            "timed": "whole call (loop upload, matter kernel, totals read back) with CUDA events",
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk else "fallback 6650 GB/s"}
 
 

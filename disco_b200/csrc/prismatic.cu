@@ -9,13 +9,14 @@
 // reference's own contracted build selects the same sets.
 //
 // The step is one cooperative kernel (matter_kernel): a first phase computes
-// every atom's slab mask once (bounding-box culling per 128-atom segment, an
-// FP32 pre-test, the exact FP64 predicate for the rest) and counts per CTA;
-// after a grid barrier the CTAs' counts are scanned per category; after a
-// second barrier the survivors are compacted in order (x, y, z and the
-// new-index map; the positions come back from L2) and the slab entries and
-// interstitial copies written in loop order, then atom order, with copies of
-// removed atoms dropped and their sources renumbered.
+// every atom's slab mask once (FP32 bounding-box culling per 128-atom
+// segment, an FP32 pre-test, the exact FP64 predicate for the rest, segments
+// spread round-robin over the grid's warps); after a grid barrier each CTA
+// counts its contiguous range, after a second the CTAs' counts are scanned
+// per category, and after a third the survivors are compacted in order (x, y,
+// z and the new-index map; the positions come back from L2) and the slab
+// entries and interstitial copies written in loop order, then atom order,
+// with copies of removed atoms dropped and their sources renumbered.
 #include <algorithm>
 #include <cmath>
 #include <cstddef>
@@ -148,7 +149,7 @@ struct SlabHead {
     float inv_df, margin;  // 1 / spacing, margin in planes
     float tlo, thi;        // slab bounds in planes
     int32_t type;          // DISCO_MATTER_VACANCY or DISCO_MATTER_INTERSTITIAL
-    int32_t pad;
+    float boundf;          // bound in FP32, rounded up (the culling)
 };
 static_assert(sizeof(SlabHead) == 80, "slab header layout");
 
@@ -164,16 +165,14 @@ constexpr int kMatterThreads = 256;
 constexpr int kMatterWarps = kMatterThreads / 32;
 constexpr int kSegRounds = 4;                                  // rounds of 32 atoms per segment
 constexpr int kSegAtoms = 32 * kSegRounds;                     // 128 atoms: one warp's unit of work
-constexpr int kChunkSegs = 32;                                 // segments per chunk of the second phase
-constexpr int kSegRow = 2 * kMaxSlabLoops;                     // per-loop slab and copy counts of a segment
+constexpr int kGroupSegs = 32;                                 // segments per warp between two flushes
+constexpr int kSegRow = 2 * kMaxSlabLoops;                     // per-loop slab and copy counts
 constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // categories counted per CTA
-constexpr int kWarpQueue = 128;                                // exact tests queued per warp
+constexpr int kWarpQueue = 512;                                // exact tests queued per warp
 constexpr int kMaxGrid = 8 * 148;                              // CTAs of one call at most
-// dynamic shared memory: per warp the masks and sides of its segment (first
-// phase), then the per-loop counts of a chunk's segments (second phase)
+constexpr int kCtlWords = 4;                                   // control words before the per-loop totals
+// dynamic shared memory: per warp the masks and sides of one segment
 constexpr size_t kMatterSmem = kMatterWarps * 2 * kSegAtoms * sizeof(uint64_t);
-static_assert(kChunkSegs * kSegRow * sizeof(int) <= kMatterSmem, "chunk counts fit the mask buffer");
-static_assert(kChunkSegs % kMatterWarps == 0, "whole rows of segments per chunk");
 
 struct MatterArgs {
     const double *x, *y, *z;
@@ -183,7 +182,7 @@ struct MatterArgs {
     int32_t nl, C;                // C = 2 + 2 nl categories: survivors, members, slab of
                                   // loop l (2 + l), kept copies of loop l (2 + nl + l)
     double Lx, Ly, Lz;
-    float iLx, iLy, iLz;          // 1 / box lengths in FP32 (the pre-test only)
+    float iLx, iLy, iLz;          // 1 / box lengths in FP32 (culling and pre-test)
     int32_t G;                    // CTAs, all resident at once (cooperative launch)
     double idLx, idLy, idLz;      // 1 / box lengths, rounded (the exact test's fast path)
     int64_t S;                    // segments of kSegAtoms atoms
@@ -192,8 +191,9 @@ struct MatterArgs {
     int32_t* seg_off;             // [S] first member record of the segment
     int32_t* cta_tot;             // [G][C] counts per CTA
     int32_t* cta_pre;             // [G][C] exclusive prefixes over the CTAs
-    unsigned int* ctl;            // [4] barrier arrivals, exits, member records taken, error word;
-                                  // zero at entry, left zero by the last CTA to leave
+    unsigned int* ctl;            // [kCtlWords] barrier arrivals, exits, member records taken, error
+                                  // word, then [2 nl] per-loop slab and kept-copy totals; zero at
+                                  // entry, left zero by the last CTA to leave
     MemberRec* members;
     int64_t member_cap;
     double *xo, *yo, *zo;
@@ -204,6 +204,8 @@ struct MatterArgs {
     disco_copy* copies;
     int64_t copy_cap;
     int64_t* totals;              // [C + 1] category totals, then the error word
+    int32_t vec_in;               // x, y, z 16-byte aligned: pairs of atoms per 16-byte load
+    int32_t vec_out;              // x_out, y_out, z_out 16-byte and new_index 8-byte aligned
 };
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
@@ -238,6 +240,18 @@ __device__ __forceinline__ double ld_hint(const double* p, uint64_t pol)
     return v;
 }
 
+__device__ __forceinline__ void ld2_hint(const double* p, uint64_t pol, double& v0, double& v1)
+{
+    asm("ld.global.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;" : "=d"(v0), "=d"(v1) : "l"(p), "l"(pol));
+}
+
+// L2 prefetch of one line (the first phase's reads follow within a few
+// microseconds; evict-last like those reads).
+__device__ __forceinline__ void prefetch_l2_keep(const void* p)
+{
+    asm volatile("prefetch.global.L2::evict_last [%0];" :: "l"(p));
+}
+
 // All CTAs of the launch arrive, then wait until `target` arrivals are
 // counted (the launch is cooperative, so every CTA is resident).  Bounded: a
 // wait that sees no progress for 2 s records DISCO_ETIMEOUT and goes on.
@@ -248,6 +262,7 @@ __device__ __forceinline__ void grid_sync(unsigned* arrive, unsigned target, int
         __threadfence();
         atomicAdd(arrive, 1u);
         unsigned long long t0 = 0;
+        unsigned sleep = 32;
         while (ld_acquire_u32(arrive) < target) {
             if (t0 == 0) {
                 t0 = global_ns();
@@ -255,7 +270,8 @@ __device__ __forceinline__ void grid_sync(unsigned* arrive, unsigned target, int
                 report(err, DISCO_ETIMEOUT);
                 break;
             }
-            __nanosleep(32);
+            __nanosleep(sleep);
+            if (sleep < 256) sleep *= 2;
         }
         __threadfence();
     }
@@ -290,26 +306,30 @@ __device__ __forceinline__ bool clearly_outside(const SlabHead& S, const float (
     return sure && (t < S.tlo - S.margin || t >= S.thi + S.margin);
 }
 
-// Smallest |p - c - m L| over p in [lo, hi] and integers m, less a rounding
-// allowance (never above the true value).
-__device__ __forceinline__ double periodic_gap(double lo, double hi, double c, double L)
+// Smallest |p - c - m L| over p in [lo, hi] and integers m, in FP32 for the
+// culling: lo, hi are the FP32 roundings of a segment's extreme coordinates,
+// c and L those of the loop centre and the box.  Every rounding is covered by
+// subtracting 1e-5 (|a| + |b| + L) + 1e-3 A (above ten times the worst
+// accumulated error of these few operations at |a| <= 1e5 L); a nearest-image
+// index off by one only lowers the result or gives 0, and beyond
+// |a| = 1e5 L (or NaN) the answer is 0.  Never above the true gap, so culling
+// with it never drops a member.
+__device__ __forceinline__ float periodic_gap_f(float lo, float hi, float c, float L, float iL)
 {
-    const double a = lo - c, b = hi - c;
-    if (!(b - a < L)) return 0.0;
-    const double m1 = floor(a / L);
-    if ((m1 + 1.0) * L <= b) return 0.0;
-    const double d = fmin(a - m1 * L, (m1 + 1.0) * L - b);
-    return fmax(0.0, d - 1e-9 * L - 1e-6);
+    const float a = lo - c, b = hi - c;
+    if (!(b - a < L) || !(fabsf(a) < 1e5f * L)) return 0.0f;
+    const float m1 = floorf(a * iL);
+    if ((m1 + 1.0f) * L <= b) return 0.0f;
+    const float d = fminf(a - m1 * L, (m1 + 1.0f) * L - b);
+    return fmaxf(0.0f, d - (1e-5f * (fabsf(a) + fabsf(b) + L) + 1e-3f));
 }
 
-// The loops among `cand` (loops whose slab can reach the atom's warp) that the
-// FP32 pre-test cannot exclude for this atom: its exact-test candidates.
-__device__ __forceinline__ uint64_t pretest(const SlabHead* sh, uint64_t cand, double x, double y, double z,
-                                            const MatterArgs& a)
+// The loops among `cand` (loops whose slab can reach the atom's segment) that
+// the FP32 pre-test cannot exclude for the atom at p (its position rounded to
+// FP32): its exact-test candidates.
+__device__ __forceinline__ uint64_t pretest(const SlabHead* sh, uint64_t cand, const float (&p)[3],
+                                            const float (&L)[3], const float (&iL)[3])
 {
-    const float L[3] = { (float)a.Lx, (float)a.Ly, (float)a.Lz };
-    const float iL[3] = { a.iLx, a.iLy, a.iLz };
-    const float p[3] = { (float)x, (float)y, (float)z };
     uint64_t c2 = 0;
     for (uint64_t c = cand; c; c &= c - 1) {
         const int l = __ffsll((long long)c) - 1;
@@ -318,28 +338,61 @@ __device__ __forceinline__ uint64_t pretest(const SlabHead* sh, uint64_t cand, d
     return c2;
 }
 
-// Survivors of one segment at their final ranks (x, y, z and the new-index
-// map); `sb` = survivors before the segment.  A segment with removed atoms
-// reads its member records for the removed ones' positions.
-__device__ __forceinline__ void copy_segment(const MatterArgs& a, int64_t s, int64_t sb, int srem, int m, int off,
-                                             uint64_t pol, int lane)
+// Streaming layout of a segment: lane t holds the atoms 64 (q / 2) + 2 t + q % 2,
+// q = 0..3 (two 16-byte loads of pairs per coordinate).
+__device__ __forceinline__ int slot_of(int q, int lane) { return 64 * (q >> 1) + 2 * lane + (q & 1); }
+
+// 16-byte streaming store of two doubles.
+__device__ __forceinline__ void st2_cs(double* p, double v0, double v1)
+{
+    __stcs(reinterpret_cast<double2*>(p), make_double2(v0, v1));
+}
+
+// One coordinate of a member-free segment in the slot_of layout (v[0..3])
+// stored at out + sb + slot with 16-byte stores; for an odd sb each lane
+// stores its second atom with the next lane's first (the pair after lane 31
+// of the first half is lane 0's first atom of the second half), lane 0 the
+// segment's first atom and lane 31 its last alone.
+__device__ __forceinline__ void store_shifted(double* out, int64_t sb, const double (&v)[kSegRounds], int lane)
+{
+    if ((sb & 1) == 0) {
+        st2_cs(out + sb + 2 * lane, v[0], v[1]);
+        st2_cs(out + sb + 64 + 2 * lane, v[2], v[3]);
+        return;
+    }
+    const double n0 = __shfl_down_sync(0xffffffffu, v[0], 1);
+    const double n2 = __shfl_down_sync(0xffffffffu, v[2], 1);
+    const double h2 = __shfl_sync(0xffffffffu, v[2], 0);
+    st2_cs(out + sb + 2 * lane + 1, v[1], lane == 31 ? h2 : n0);
+    if (lane < 31) st2_cs(out + sb + 64 + 2 * lane + 1, v[3], n2);
+    else __stcs(out + sb + kSegAtoms - 1, v[3]);
+    if (lane == 0) __stcs(out + sb, v[0]);
+}
+
+// Member-free segment: every atom survives, the survivors are the segment
+// shifted to `sb` (survivors before it).  Whole segments with aligned arrays
+// move in 16-byte loads and stores.
+__device__ __forceinline__ void copy_plain(const MatterArgs& a, int64_t s, int64_t sb, uint64_t pol, int lane)
 {
     const int64_t i0 = s * kSegAtoms;
-    unsigned rb[kSegRounds];
+    if (a.vec_in && a.vec_out && i0 + kSegAtoms <= a.n && sb >= 0 && sb + kSegAtoms <= a.n) {
+        double x[kSegRounds], y[kSegRounds], z[kSegRounds];
 #pragma unroll
-    for (int r = 0; r < kSegRounds; ++r) rb[r] = 0u;
-    if (srem > 0 && (int64_t)off + m <= a.member_cap) {
-        for (int e0 = 0; e0 < m; e0 += 32) {
-            const int e = e0 + lane;
-            unsigned li = 0xffffffffu;
-            if (e < m) {
-                const MemberRec* rec = a.members + off + e;
-                if (__ldcg(&rec->removed)) li = (unsigned)(__ldcg(&rec->atom) - i0);
-            }
-#pragma unroll
-            for (int r = 0; r < kSegRounds; ++r)
-                rb[r] |= __reduce_or_sync(0xffffffffu, (li >> 5) == (unsigned)r ? 1u << (li & 31u) : 0u);
+        for (int h = 0; h < 2; ++h) {
+            const int64_t i = i0 + 64 * h + 2 * lane;
+            ld2_hint(a.x + i, pol, x[2 * h], x[2 * h + 1]);
+            ld2_hint(a.y + i, pol, y[2 * h], y[2 * h + 1]);
+            ld2_hint(a.z + i, pol, z[2 * h], z[2 * h + 1]);
         }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int32_t q = (int32_t)(sb + 64 * h + 2 * lane);
+            __stcs(reinterpret_cast<int2*>(a.new_index + i0 + 64 * h + 2 * lane), make_int2(q, q + 1));
+        }
+        store_shifted(a.xo, sb, x, lane);
+        store_shifted(a.yo, sb, y, lane);
+        store_shifted(a.zo, sb, z, lane);
+        return;
     }
     double px[kSegRounds], py[kSegRounds], pz[kSegRounds];
 #pragma unroll
@@ -348,7 +401,99 @@ __device__ __forceinline__ void copy_segment(const MatterArgs& a, int64_t s, int
         px[r] = py[r] = pz[r] = 0.0;
         if (i < a.n) { px[r] = ld_hint(a.x + i, pol); py[r] = ld_hint(a.y + i, pol); pz[r] = ld_hint(a.z + i, pol); }
     }
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) {
+        const int64_t i = i0 + r * 32 + lane;
+        const int64_t q = sb + r * 32 + lane;
+        if (i < a.n && q >= 0 && q < a.n) {
+            __stcs(a.xo + q, px[r]); __stcs(a.yo + q, py[r]); __stcs(a.zo + q, pz[r]);
+            __stcs(a.new_index + i, (int32_t)q);
+        }
+    }
+}
+
+// Segment with slab members (its m records at `rec`): the records' masks and
+// sides go back into the warp's per-slot table (smask / ssides), then per
+// loop its slab entries and interstitial copies at the warp's running
+// positions wrun[l] / wrun[nl + l] (ascending atom order within the loop;
+// copies of removed atoms dropped, sources renumbered), then the survivors,
+// the removed atoms skipped.
+__device__ __forceinline__ void copy_members(const MatterArgs& a, const SlabHead* sh, uint64_t vac, int64_t s,
+                                             int64_t sb, const MemberRec* rec, int m, uint64_t* smask,
+                                             uint64_t* ssides, int64_t* wrun, uint64_t pol, int lane)
+{
+    const int64_t i0 = s * kSegAtoms;
+    const int nl = a.nl;
     const unsigned ltm = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) { smask[r * 32 + lane] = 0; ssides[r * 32 + lane] = 0; }
+    __syncwarp();
+    for (int e = lane; e < m; e += 32) {
+        const int slot = __ldcg(&rec[e].atom) - (int)i0;
+        if (slot >= 0 && slot < kSegAtoms) {
+            smask[slot] = __ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].mask));
+            ssides[slot] = __ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].sides));
+        }
+    }
+    __syncwarp();
+    unsigned rb[kSegRounds];
+    uint64_t un = 0;
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) {
+        const uint64_t mk = smask[r * 32 + lane];
+        rb[r] = __ballot_sync(0xffffffffu, (mk & vac) != 0);
+        un |= mk;
+    }
+    un = ((uint64_t)__reduce_or_sync(0xffffffffu, (unsigned)(un >> 32)) << 32) |
+         __reduce_or_sync(0xffffffffu, (unsigned)un);
+    for (uint64_t u = un; u; u &= u - 1) {
+        const int l = __ffsll((long long)u) - 1;
+        const bool inter = sh[l].type == DISCO_MATTER_INTERSTITIAL;
+        int64_t qs = wrun[l], qc = wrun[nl + l];
+        int rem_before = 0;
+#pragma unroll
+        for (int r = 0; r < kSegRounds; ++r) {
+            const uint64_t mk = smask[r * 32 + lane];
+            const bool in = (mk >> l) & 1ull;
+            const bool removed = (rb[r] >> lane) & 1u;
+            const bool kp = in && inter && !removed;
+            const bool pos = (ssides[r * 32 + lane] >> l) & 1ull;
+            const unsigned bi = __ballot_sync(0xffffffffu, in);
+            const unsigned bk = __ballot_sync(0xffffffffu, kp);
+            if (in) {
+                const int64_t q = qs + __popc(bi & ltm);
+                if (q >= 0 && q < a.slab_cap) {
+                    a.slab_atoms[q] = (int32_t)(i0 + r * 32 + lane);
+                    a.slab_side[q] = pos ? 1 : -1;
+                }
+            }
+            if (kp) {
+                const int64_t q = qc + __popc(bk & ltm);
+                if (q >= 0 && q < a.copy_cap) {
+                    const disco_slab_loop& g = a.loops[l].L;
+                    const double* shf = pos ? g.shift_pos : g.shift_neg;
+                    disco_copy cp;
+                    cp.atom = (int32_t)(sb + r * 32 + lane - (rem_before + __popc(rb[r] & ltm)));
+                    cp.reserved = 0;
+                    cp.shift[0] = shf[0]; cp.shift[1] = shf[1]; cp.shift[2] = shf[2];
+                    a.copies[q] = cp;
+                }
+            }
+            qs += __popc(bi);
+            qc += __popc(bk);
+            rem_before += __popc(rb[r]);
+        }
+        __syncwarp();
+        if (lane == 0) { wrun[l] = qs; wrun[nl + l] = qc; }
+        __syncwarp();
+    }
+    double px[kSegRounds], py[kSegRounds], pz[kSegRounds];
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) {
+        const int64_t i = i0 + r * 32 + lane;
+        px[r] = py[r] = pz[r] = 0.0;
+        if (i < a.n) { px[r] = ld_hint(a.x + i, pol); py[r] = ld_hint(a.y + i, pol); pz[r] = ld_hint(a.z + i, pol); }
+    }
     int before = 0;
 #pragma unroll
     for (int r = 0; r < kSegRounds; ++r) {
@@ -364,59 +509,148 @@ __device__ __forceinline__ void copy_segment(const MatterArgs& a, int64_t s, int
         }
         before += __popc(rb[r]);
     }
+    __syncwarp();                                               // the table is rewritten
 }
 
-// Union of the slab masks of a segment's m member records (warp-wide).
-__device__ __forceinline__ uint64_t segment_union(const MemberRec* rec, int m, int lane)
+// From the masks and sides of segment s in the warp's shared-memory buffer:
+// its removed and member counts, the per-loop slab and kept-copy counts
+// (added to wcnt), and its member records in atom order at `off` (taken here
+// from the global record counter when off < 0).
+__device__ __forceinline__ void aggregate_segment(const MatterArgs& a, const SlabHead* sh, uint64_t vac, int64_t s,
+                                                  const uint64_t* smask, const uint64_t* ssides, int* wcnt,
+                                                  int& rc, int& mc, int& off, int lane)
 {
-    uint64_t u = 0;
-    for (int e = lane; e < m; e += 32) u |= __ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].mask));
-    const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)u);
-    const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(u >> 32));
-    return ((uint64_t)hi << 32) | lo;
+    const int64_t i0 = s * kSegAtoms;
+    const int nl = a.nl;
+    const unsigned ltm = (1u << lane) - 1u;
+    unsigned bm[kSegRounds];
+    rc = 0;
+    mc = 0;
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) {
+        const uint64_t mask = smask[r * 32 + lane];
+        const bool removed = (mask & vac) != 0;
+        bm[r] = __ballot_sync(0xffffffffu, mask != 0);
+        rc += __popc(__ballot_sync(0xffffffffu, removed));
+        mc += __popc(bm[r]);
+        for (uint64_t u = mask; u; u &= u - 1) {             // members are rare
+            const int l = __ffsll((long long)u) - 1;
+            atomicAdd(&wcnt[l], 1);
+            if (sh[l].type == DISCO_MATTER_INTERSTITIAL && !removed) atomicAdd(&wcnt[nl + l], 1);
+        }
+    }
+    if (off < 0) {
+        int o = 0;
+        if (lane == 0 && mc > 0) o = (int)atomicAdd(a.ctl + 2, (unsigned)mc);
+        off = __shfl_sync(0xffffffffu, o, 0);
+    }
+    int e = off;
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) {
+        const uint64_t mask = smask[r * 32 + lane];
+        if (mask) {
+            const int64_t q = (int64_t)e + __popc(bm[r] & ltm);
+            if (q < a.member_cap) {
+                MemberRec rec;
+                rec.atom = (int32_t)(i0 + r * 32 + lane);
+                rec.removed = (mask & vac) != 0;
+                rec.mask = mask;
+                rec.sides = ssides[r * 32 + lane];
+                a.members[q] = rec;
+            }
+        }
+        e += __popc(bm[r]);
+    }
 }
 
-// The matter step in one cooperative launch.  CTA k owns a contiguous range
-// of 128-atom segments; its warps take every eighth segment of it.
-//   Phase 1 (positions from HBM, kept in L2): per segment the bounding box of
-//     its atoms, the loops whose slab can reach it, and for those (rare)
-//     segments the FP32 pre-test and the exact FP64 tests of the candidate
-//     (atom, loop) pairs queued per warp and spread over its lanes; the
-//     segment's member records are written in atom order into a block taken
-//     from a global counter, and per segment its removed and member counts;
-//     per CTA the counts of every category.
-//   Grid barrier; CTA c scans category c over the CTAs; grid barrier.
-//   Phase 2 (positions again, from L2): per chunk of 32 segments, the warps
-//     copy the survivors of their segments to their final ranks (a segment
-//     without removed atoms is a shifted copy), and when the chunk holds slab
-//     members the CTA writes their slab entries and interstitial copies in
-//     atom order at loop base + CTA prefix + chunk prefix + rank (loop order,
-//     then slab order: Code/prismatic.cpp:61-72, Code/main.cpp:651-654,676-679).
-// No look-back and no second kernel: the only waits are the two barriers.
+// A segment whose candidates do not fit the warp's queue: its exact tests
+// lane by lane, then its counts and records (out of line: a rare path that
+// would otherwise raise the register count of the streaming loop; `a` lives
+// in shared memory).  Returns (removed, members, first record).
+__device__ __noinline__ int3 direct_segment(const MatterArgs& a, const SlabHead* sh, uint64_t vac, int64_t s,
+                                           uint64_t c0, uint64_t c1, uint64_t c2, uint64_t c3, uint64_t* smask,
+                                           uint64_t* ssides, int* wcnt, int lane)
+{
+    const int64_t i0 = s * kSegAtoms;
+    const uint64_t cand[kSegRounds] = { c0, c1, c2, c3 };
+#pragma unroll
+    for (int r = 0; r < kSegRounds; ++r) { smask[r * 32 + lane] = 0; ssides[r * 32 + lane] = 0; }
+    __syncwarp();
+#pragma unroll 1
+    for (int q = 0; q < kSegRounds; ++q) {
+        const int slot = slot_of(q, lane);
+        const int64_t i = i0 + slot;
+        for (uint64_t c = cand[q]; c; c &= c - 1) {
+            const int l = __ffsll((long long)c) - 1;
+            bool ps = false;
+            if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy, a.idLz, ps)) {
+                smask[slot] |= 1ull << l;
+                if (ps) ssides[slot] |= 1ull << l;
+            }
+        }
+    }
+    __syncwarp();
+    int rc = 0, mc = 0, off = -1;
+    aggregate_segment(a, sh, vac, s, smask, ssides, wcnt, rc, mc, off, lane);
+    __syncwarp();
+    return make_int3(rc, mc, mc > 0 ? off : 0);
+}
+
+// The matter step in one cooperative launch.
+//   Phase 1, masks.  The grid's warps take the 128-atom segments round-robin
+//     (warp g takes g, g + W, g + 2 W, ...), so that loops clustered in space
+//     load every SM alike.  Per segment: the positions (16-byte loads,
+//     prefetched two segments ahead, kept in L2 for phase 2) rounded to FP32
+//     for a bounding box and a per-loop cull; for the few segments a loop can
+//     reach, the FP32 pre-test per atom, its candidate (atom, loop) pairs
+//     queued per warp.  After every 32 segments the warp runs the exact FP64
+//     tests of its queue spread over its lanes, then per listed segment the
+//     masks, counts and member records (atom order, one block of records per
+//     flush).  Per segment: removed and member counts, first record; per
+//     call: the per-loop slab and kept-copy totals.
+//   Barrier; per CTA, its counts from the per-segment results, per warp of
+//     its contiguous range; barrier; CTA c scans category c over the CTAs;
+//     barrier.
+//   Phase 2, ordered writes.  CTA k owns a contiguous range of segments, cut
+//     into eight contiguous warp ranges; each warp walks its range with the
+//     running survivor rank: a member-free segment is a shifted copy; a
+//     segment with members writes their slab entries and copies at the warp's
+//     running per-loop positions (loop base + CTA prefix + earlier warps'
+//     counts), in atom order (Code/prismatic.cpp:61-72,
+//     Code/main.cpp:651-654,676-679), then its survivors.
+// No look-back and no second kernel: the only waits are the three barriers.
 // The outputs must not overlap the positions.
-__global__ void __launch_bounds__(kMatterThreads, 4) matter_kernel(const MatterArgs a)
+__global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterArgs a)
 {
-    extern __shared__ __align__(16) unsigned char dyn[];
+    extern __shared__ __align__(16) unsigned char dyn[];       // per warp: masks and sides of one segment
     __shared__ SlabHead sh[kMaxSlabLoops];
-    __shared__ int cnt_c[kMaxCats];                             // this CTA's counts per category
-    __shared__ int wq[kMatterWarps][kWarpQueue];                // per warp: (slot, loop) pairs to test
-    __shared__ int wq_n[kMatterWarps];
-    __shared__ int64_t run[kSegRow];                            // phase 2: next slab entry / copy per loop
-    __shared__ int ctot[kSegRow];                               // phase 2: a chunk's counts per loop category
+    __shared__ __align__(16) unsigned char wq_raw[kMatterWarps * kWarpQueue * 4];   // phase 1 queues, phase 2 wrun
+    __shared__ int wl_seg[kMatterWarps][kGroupSegs];           // listed segments of a group (index in the group)
+    __shared__ int wl_q[kMatterWarps][kGroupSegs];             // their first queue entry | count << 16
+    __shared__ int wl_mr[kMatterWarps][kGroupSegs];            // their member count | removed count << 16
+    __shared__ int wcnt[kMatterWarps][kSegRow];                // per warp: slab / kept-copy counts per loop
+    __shared__ int wrem[kMatterWarps], wmem[kMatterWarps];
+    __shared__ int64_t run[kSegRow];                           // CTA's first slab entry / copy per loop
     __shared__ int64_t scan_w[kMatterWarps];
     __shared__ unsigned long long vac_s;
+    __shared__ MatterArgs sa;                                  // for the out-of-line rare path
+    static_assert(kMatterWarps * kSegRow * sizeof(int64_t) <= sizeof(wq_raw), "phase 2 positions fit the queues");
+    static_assert(sizeof(MatterArgs) % 8 == 0, "argument block copied in words");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nl = a.nl, C = a.C, G = a.G;
     const int64_t k = blockIdx.x;
     const int64_t seg_lo = k * a.S / G, seg_hi = (k + 1) * a.S / G;
+    const int64_t nseg = seg_hi - seg_lo;
+    const int64_t wlo = seg_lo + nseg * warp / kMatterWarps, whi = seg_lo + nseg * (warp + 1) / kMatterWarps;
     int* err = reinterpret_cast<int*>(a.ctl + 3);
-    const unsigned ltm = (1u << lane) - 1u;
     {
         const int words = nl * (int)(sizeof(SlabHead) / 8);
         const uint64_t* src = reinterpret_cast<const uint64_t*>(a.heads);
         uint64_t* dst = reinterpret_cast<uint64_t*>(sh);
         for (int i = tid; i < words; i += kMatterThreads) dst[i] = src[i];
-        for (int i = tid; i < C; i += kMatterThreads) cnt_c[i] = 0;
+        for (int i = lane; i < 2 * nl; i += 32) wcnt[warp][i] = 0;
+        const uint64_t* as = reinterpret_cast<const uint64_t*>(&a);
+        for (int i = tid; i < (int)(sizeof(MatterArgs) / 8); i += kMatterThreads) reinterpret_cast<uint64_t*>(&sa)[i] = as[i];
         if (tid == 0) vac_s = 0ull;
     }
     __syncthreads();
@@ -424,141 +658,253 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_kernel(const MatterA
     __syncthreads();
     const uint64_t vac = vac_s;
 
-    // ---- phase 1: masks and counts --------------------------------------------------
+    // ---- phase 1: masks --------------------------------------------------------------
     {
         const uint64_t keep = l2_policy_keep();
+        uint32_t* wq = reinterpret_cast<uint32_t*>(wq_raw) + warp * kWarpQueue;
         uint64_t* smask = reinterpret_cast<uint64_t*>(dyn) + warp * (2 * kSegAtoms);
         uint64_t* ssides = smask + kSegAtoms;
-        int w_removed = 0, w_members = 0;
-        for (int64_t s = seg_lo + warp; s < seg_hi; s += kMatterWarps) {
-            const int64_t i0 = s * kSegAtoms;
-            double lo[3] = { 1e300, 1e300, 1e300 }, hi[3] = { -1e300, -1e300, -1e300 };
-            {
-                double px[kSegRounds], py[kSegRounds], pz[kSegRounds];
-#pragma unroll
-                for (int r = 0; r < kSegRounds; ++r) {
-                    const int64_t i = i0 + r * 32 + lane;
-                    px[r] = py[r] = pz[r] = 0.0;
-                    if (i < a.n) { px[r] = ld_hint(a.x + i, keep); py[r] = ld_hint(a.y + i, keep); pz[r] = ld_hint(a.z + i, keep); }
+        const double* pf_base = lane < 8 ? a.x : lane < 16 ? a.y : a.z;
+        const float Lf[3] = { (float)a.Lx, (float)a.Ly, (float)a.Lz };
+        const float iLf[3] = { a.iLx, a.iLy, a.iLz };
+        const int64_t W = (int64_t)G * kMatterWarps, gw = k * kMatterWarps + warp;
+        const int64_t nj = gw < a.S ? (a.S - 1 - gw) / W + 1 : 0;
+        for (int64_t j0 = 0; j0 < nj; j0 += kGroupSegs) {
+            const int64_t j1 = nj - j0 < kGroupSegs ? nj : j0 + kGroupSegs;
+            int nq = 0, nlst = 0;
+            for (int64_t j = j0; j < j1; ++j) {
+                const int64_t s = gw + j * W;
+                const int64_t i0 = s * kSegAtoms;
+                if (lane < 24 && j + 2 < nj) {
+                    const int64_t pi = (s + 2 * W) * kSegAtoms + (lane & 7) * 16;
+                    if (pi < a.n) prefetch_l2_keep(pf_base + pi);
                 }
+                // the segment's positions rounded to FP32 (slot_of layout); an
+                // atom past n repeats the segment's first atom
+                float fx[kSegRounds], fy[kSegRounds], fz[kSegRounds];
+                if (a.vec_in && i0 + kSegAtoms <= a.n) {
 #pragma unroll
-                for (int r = 0; r < kSegRounds; ++r)
-                    if (i0 + r * 32 + lane < a.n) {
-                        lo[0] = fmin(lo[0], px[r]); hi[0] = fmax(hi[0], px[r]);
-                        lo[1] = fmin(lo[1], py[r]); hi[1] = fmax(hi[1], py[r]);
-                        lo[2] = fmin(lo[2], pz[r]); hi[2] = fmax(hi[2], pz[r]);
+                    for (int h = 0; h < 2; ++h) {
+                        const int64_t i = i0 + 64 * h + 2 * lane;
+                        double x0, x1, y0, y1, z0, z1;
+                        ld2_hint(a.x + i, keep, x0, x1);
+                        ld2_hint(a.y + i, keep, y0, y1);
+                        ld2_hint(a.z + i, keep, z0, z1);
+                        fx[2 * h] = (float)x0; fx[2 * h + 1] = (float)x1;
+                        fy[2 * h] = (float)y0; fy[2 * h + 1] = (float)y1;
+                        fz[2 * h] = (float)z0; fz[2 * h + 1] = (float)z1;
                     }
-            }
-            uint64_t wmask = 0;
-            if (nl > 0) {
+                } else {
 #pragma unroll
-                for (int d = 0; d < 3; ++d)
-                    for (int o = 16; o > 0; o >>= 1) {
-                        lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-                        hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+                    for (int q = 0; q < kSegRounds; ++q) {
+                        int64_t i = i0 + slot_of(q, lane);
+                        if (i >= a.n) i = i0;
+                        fx[q] = (float)ld_hint(a.x + i, keep);
+                        fy[q] = (float)ld_hint(a.y + i, keep);
+                        fz[q] = (float)ld_hint(a.z + i, keep);
                     }
-                for (int half = 0; half * 32 < nl; ++half) {
-                    const int l = lane + 32 * half;
-                    bool reach = false;
-                    if (l < nl) {
-                        const SlabHead& S = sh[l];
-                        const double gx = periodic_gap(lo[0], hi[0], S.cx, a.Lx);
-                        const double gy = periodic_gap(lo[1], hi[1], S.cy, a.Ly);
-                        const double gz = periodic_gap(lo[2], hi[2], S.cz, a.Lz);
-                        reach = !(gx * gx + gy * gy + gz * gz > S.bound * S.bound);
-                    }
-                    wmask |= (uint64_t)__ballot_sync(0xffffffffu, reach) << (32 * half);
                 }
-            }
-            int rc = 0, mc = 0, off = 0;
-            if (wmask) {
-                // the pre-test per atom, its candidate (atom, loop) pairs queued,
-                // the exact tests of the queue spread over the lanes
+                // the loops whose slab can reach the segment's bounding box
+                uint64_t wmask = 0;
+                if (nl > 0) {
+                    float lo[3] = { fminf(fminf(fx[0], fx[1]), fminf(fx[2], fx[3])),
+                                    fminf(fminf(fy[0], fy[1]), fminf(fy[2], fy[3])),
+                                    fminf(fminf(fz[0], fz[1]), fminf(fz[2], fz[3])) };
+                    float hi[3] = { fmaxf(fmaxf(fx[0], fx[1]), fmaxf(fx[2], fx[3])),
+                                    fmaxf(fmaxf(fy[0], fy[1]), fmaxf(fy[2], fy[3])),
+                                    fmaxf(fmaxf(fz[0], fz[1]), fmaxf(fz[2], fz[3])) };
 #pragma unroll
-                for (int r = 0; r < kSegRounds; ++r) { smask[r * 32 + lane] = 0; ssides[r * 32 + lane] = 0; }
-                if (lane == 0) wq_n[warp] = 0;
-                __syncwarp();
-#pragma unroll 1
-                for (int r = 0; r < kSegRounds; ++r) {
-                    const int64_t i = i0 + r * 32 + lane;
-                    uint64_t cand = 0;
-                    if (i < a.n) cand = pretest(sh, wmask, a.x[i], a.y[i], a.z[i], a);
-                    for (uint64_t c = cand; c; c &= c - 1) {
-                        const int l = __ffsll((long long)c) - 1;
-                        const int q = atomicAdd(&wq_n[warp], 1);
-                        if (q < kWarpQueue) {
-                            wq[warp][q] = (r * 32 + lane) | (l << 16);
-                        } else {                                 // a full queue: test here
-                            bool ps = false;
-                            if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy,
-                                            a.idLz, ps)) {
-                                atomicOr(reinterpret_cast<unsigned long long*>(&smask[r * 32 + lane]), 1ull << l);
-                                if (ps) atomicOr(reinterpret_cast<unsigned long long*>(&ssides[r * 32 + lane]), 1ull << l);
-                            }
+                    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                            hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+                        }
+                    for (int half = 0; half * 32 < nl; ++half) {
+                        const int l = lane + 32 * half;
+                        bool reach = false;
+                        if (l < nl) {
+                            const SlabHead& S = sh[l];
+                            const float gx = periodic_gap_f(lo[0], hi[0], S.cf[0], Lf[0], iLf[0]);
+                            const float gy = periodic_gap_f(lo[1], hi[1], S.cf[1], Lf[1], iLf[1]);
+                            const float gz = periodic_gap_f(lo[2], hi[2], S.cf[2], Lf[2], iLf[2]);
+                            reach = !(gx * gx + gy * gy + gz * gz > S.boundf * S.boundf);
+                        }
+                        wmask |= (uint64_t)__ballot_sync(0xffffffffu, reach) << (32 * half);
+                    }
+                }
+                int rc = 0, mc = 0, off = 0;
+                bool listed = false;
+                if (wmask) {
+                    // the FP32 pre-test per atom: its exact-test candidates
+                    uint64_t cand[kSegRounds];
+                    int cnt = 0;
+#pragma unroll
+                    for (int q = 0; q < kSegRounds; ++q) {
+                        const float p[3] = { fx[q], fy[q], fz[q] };
+                        cand[q] = i0 + slot_of(q, lane) < a.n ? pretest(sh, wmask, p, Lf, iLf) : 0ull;
+                        cnt += __popcll(cand[q]);
+                    }
+                    int pre = cnt;
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int y = __shfl_up_sync(0xffffffffu, pre, o);
+                        if (lane >= o) pre += y;
+                    }
+                    const int T = __shfl_sync(0xffffffffu, pre, 31);
+                    pre -= cnt;
+                    if (T > 0 && nq + T <= kWarpQueue) {
+                        // queued: (loop, slot, segment of the group), tested at the flush
+                        int q = nq + pre;
+#pragma unroll
+                        for (int r = 0; r < kSegRounds; ++r)
+                            for (uint64_t c = cand[r]; c; c &= c - 1)
+                                wq[q++] = (uint32_t)(__ffsll((long long)c) - 1) | ((uint32_t)slot_of(r, lane) << 6) |
+                                          ((uint32_t)(j - j0) << 13);
+                        if (lane == 0) {
+                            wl_seg[warp][nlst] = (int)(j - j0);
+                            wl_q[warp][nlst] = nq | (T << 16);
+                        }
+                        nq += T;
+                        ++nlst;
+                        listed = true;
+                    } else if (T > 0) {
+                        // the queue is full: this segment's exact tests here, lane by lane
+                        const int3 res = direct_segment(sa, sh, vac, s, cand[0], cand[1], cand[2], cand[3], smask,
+                                                        ssides, wcnt[warp], lane);
+                        rc = res.x;
+                        mc = res.y;
+                        off = res.z;
+                    }
+                }
+                if (!listed && lane == 0) { a.seg_removed[s] = rc; a.seg_members[s] = mc; a.seg_off[s] = off; }
+            }
+            if (nq == 0) continue;
+            // flush: the exact tests of the queue spread over the lanes, the
+            // result in bits 29 (member) and 30 (positive side) of each entry
+            __syncwarp();
+            for (int q = lane; q < nq; q += 32) {
+                const uint32_t e = wq[q];
+                const int l = e & 63, slot = (e >> 6) & 127;
+                const int64_t i = (gw + (j0 + (e >> 13)) * W) * kSegAtoms + slot;
+                bool ps = false;
+                const bool in = slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy,
+                                            a.idLz, ps);
+                wq[q] = e | (in ? 1u << 29 : 0u) | (ps ? 1u << 30 : 0u);
+            }
+            __syncwarp();
+            // member and removed counts per listed segment, then one block of records
+            int tot = 0;
+            for (int jj = 0; jj < nlst; ++jj) {
+                const int qo = wl_q[warp][jj] & 0xffff, qn = wl_q[warp][jj] >> 16;
+                unsigned mb[kSegRounds], rbm[kSegRounds];
+#pragma unroll
+                for (int r = 0; r < kSegRounds; ++r) { mb[r] = 0u; rbm[r] = 0u; }
+                for (int q0 = 0; q0 < qn; q0 += 32) {
+                    unsigned slot = 0xffffffffu;
+                    bool rmv = false;
+                    if (q0 + lane < qn) {
+                        const uint32_t e = wq[qo + q0 + lane];
+                        if (e & (1u << 29)) {
+                            slot = (e >> 6) & 127;
+                            rmv = (vac >> (e & 63)) & 1ull;
                         }
                     }
-                }
-                __syncwarp();
-                const int nq = min(wq_n[warp], kWarpQueue);
-                for (int q = lane; q < nq; q += 32) {
-                    const int slot = wq[warp][q] & 0xffff, l = wq[warp][q] >> 16;
-                    const int64_t i = i0 + slot;
-                    bool ps = false;
-                    if (slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy, a.idLz, ps)) {
-                        atomicOr(reinterpret_cast<unsigned long long*>(&smask[slot]), 1ull << l);
-                        if (ps) atomicOr(reinterpret_cast<unsigned long long*>(&ssides[slot]), 1ull << l);
+#pragma unroll
+                    for (int r = 0; r < kSegRounds; ++r) {
+                        const unsigned bit = (slot >> 5) == (unsigned)r ? 1u << (slot & 31u) : 0u;
+                        mb[r] |= __reduce_or_sync(0xffffffffu, bit);
+                        rbm[r] |= __reduce_or_sync(0xffffffffu, rmv ? bit : 0u);
                     }
                 }
-                __syncwarp();
-                // counts, then the member records in atom order
-                unsigned bm[kSegRounds];
+                int m = 0, rm = 0;
 #pragma unroll
-                for (int r = 0; r < kSegRounds; ++r) {
-                    const uint64_t mask = smask[r * 32 + lane];
-                    const bool removed = (mask & vac) != 0;
-                    bm[r] = __ballot_sync(0xffffffffu, mask != 0);
-                    rc += __popc(__ballot_sync(0xffffffffu, removed));
-                    mc += __popc(bm[r]);
-                    for (uint64_t u = mask; u; u &= u - 1) {     // members are rare
-                        const int l = __ffsll((long long)u) - 1;
-                        atomicAdd(&cnt_c[2 + l], 1);
-                        if (sh[l].type == DISCO_MATTER_INTERSTITIAL && !removed) atomicAdd(&cnt_c[2 + nl + l], 1);
-                    }
-                }
-                if (lane == 0) off = (int)atomicAdd(a.ctl + 2, (unsigned)mc);
-                off = __shfl_sync(0xffffffffu, off, 0);
-                int e = off;
+                for (int r = 0; r < kSegRounds; ++r) { m += __popc(mb[r]); rm += __popc(rbm[r]); }
+                if (lane == 0) wl_mr[warp][jj] = m | (rm << 16);
+                tot += m;
+            }
+            int base = 0;
+            if (lane == 0 && tot > 0) base = (int)atomicAdd(a.ctl + 2, (unsigned)tot);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            __syncwarp();
+            for (int jj = 0; jj < nlst; ++jj) {
+                const int64_t s = gw + (j0 + wl_seg[warp][jj]) * W;
+                const int m = wl_mr[warp][jj] & 0xffff, rm = wl_mr[warp][jj] >> 16;
+                if (m > 0) {
+                    const int qo = wl_q[warp][jj] & 0xffff, qn = wl_q[warp][jj] >> 16;
 #pragma unroll
-                for (int r = 0; r < kSegRounds; ++r) {
-                    const uint64_t mask = smask[r * 32 + lane];
-                    if (mask) {
-                        const int64_t q = (int64_t)e + __popc(bm[r] & ltm);
-                        if (q < a.member_cap) {
-                            MemberRec rec;
-                            rec.atom = (int32_t)(i0 + r * 32 + lane);
-                            rec.removed = (mask & vac) != 0;
-                            rec.mask = mask;
-                            rec.sides = ssides[r * 32 + lane];
-                            a.members[q] = rec;
+                    for (int r = 0; r < kSegRounds; ++r) { smask[r * 32 + lane] = 0; ssides[r * 32 + lane] = 0; }
+                    __syncwarp();
+                    for (int q = lane; q < qn; q += 32) {
+                        const uint32_t e = wq[qo + q];
+                        if (e & (1u << 29)) {
+                            const int slot = (e >> 6) & 127;
+                            atomicOr(reinterpret_cast<unsigned long long*>(&smask[slot]), 1ull << (e & 63));
+                            if (e & (1u << 30))
+                                atomicOr(reinterpret_cast<unsigned long long*>(&ssides[slot]), 1ull << (e & 63));
                         }
                     }
-                    e += __popc(bm[r]);
+                    __syncwarp();
+                    int rc2 = 0, mc2 = 0, off2 = base;
+                    aggregate_segment(a, sh, vac, s, smask, ssides, wcnt[warp], rc2, mc2, off2, lane);
+                    __syncwarp();
                 }
+                if (lane == 0) { a.seg_removed[s] = rm; a.seg_members[s] = m; a.seg_off[s] = m > 0 ? base : 0; }
+                base += m;
             }
-            if (lane == 0) { a.seg_removed[s] = rc; a.seg_members[s] = mc; a.seg_off[s] = off; }
-            w_removed += rc;
-            w_members += mc;
+            __syncwarp();                                       // the queue is rewritten
         }
-        if (lane == 0) { atomicAdd(&cnt_c[0], w_removed); atomicAdd(&cnt_c[1], w_members); }
+        // the warp's per-loop counts into the call's per-loop totals (exact
+        // whether or not every member record found room)
+        __syncwarp();
+        for (int c = lane; c < 2 * nl; c += 32)
+            if (wcnt[warp][c]) atomicAdd(a.ctl + kCtlWords + c, (unsigned)wcnt[warp][c]);
+    }
+    grid_sync(a.ctl, (unsigned)G, err);
+
+    // ---- this CTA's counts: per warp of its contiguous range (the second
+    // phase's order) the removed and member atoms and, from the member
+    // records, the slab entries and kept copies of every loop
+    {
+        int rem = 0, mem = 0;
+        for (int i = lane; i < 2 * nl; i += 32) wcnt[warp][i] = 0;
+        __syncwarp();
+        for (int64_t c0 = wlo; c0 < whi; c0 += 32) {
+            const int cn = (int)(whi - c0 < 32 ? whi - c0 : 32);
+            const int v_rem = lane < cn ? __ldcg(a.seg_removed + c0 + lane) : 0;
+            const int v_mem = lane < cn ? __ldcg(a.seg_members + c0 + lane) : 0;
+            const int v_off = lane < cn ? __ldcg(a.seg_off + c0 + lane) : 0;
+            rem += __reduce_add_sync(0xffffffffu, v_rem);
+            mem += __reduce_add_sync(0xffffffffu, v_mem);
+            for (unsigned b = __ballot_sync(0xffffffffu, v_mem > 0); b; b &= b - 1) {
+                const int j = __ffs(b) - 1;
+                const int m = __shfl_sync(0xffffffffu, v_mem, j), off = __shfl_sync(0xffffffffu, v_off, j);
+                if ((int64_t)off + m > a.member_cap) continue;
+                for (int e = lane; e < m; e += 32) {
+                    const MemberRec* rec = a.members + off + e;
+                    const uint64_t mk = __ldcg(reinterpret_cast<const unsigned long long*>(&rec->mask));
+                    const bool removed = __ldcg(&rec->removed) != 0;
+                    for (uint64_t u = mk; u; u &= u - 1) {
+                        const int l = __ffsll((long long)u) - 1;
+                        atomicAdd(&wcnt[warp][l], 1);
+                        if (sh[l].type == DISCO_MATTER_INTERSTITIAL && !removed) atomicAdd(&wcnt[warp][nl + l], 1);
+                    }
+                }
+            }
+        }
+        if (lane == 0) { wrem[warp] = rem; wmem[warp] = mem; }
     }
     __syncthreads();
     {
         const int64_t e_hi = seg_hi * kSegAtoms < a.n ? seg_hi * kSegAtoms : a.n;
         const int64_t atoms_k = seg_hi > seg_lo ? e_hi - seg_lo * kSegAtoms : 0;
-        for (int c = tid; c < C; c += kMatterThreads)
-            a.cta_tot[k * C + c] = c == 0 ? (int32_t)(atoms_k - cnt_c[0]) : cnt_c[c];
+        for (int c = tid; c < C; c += kMatterThreads) {
+            int v = 0;
+            for (int w = 0; w < kMatterWarps; ++w)
+                v += c == 0 ? wrem[w] : c == 1 ? wmem[w] : wcnt[w][c - 2];
+            a.cta_tot[k * C + c] = c == 0 ? (int32_t)(atoms_k - v) : v;
+        }
     }
-    grid_sync(a.ctl, (unsigned)G, err);
+    grid_sync(a.ctl, 2u * (unsigned)G, err);
 
     // ---- scan: CTA c takes category c, exclusive prefixes over the CTAs --------------
     for (int c = blockIdx.x; c < C; c += G) {
@@ -585,10 +931,11 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_kernel(const MatterA
                 a.cta_pre[(int64_t)(k0 + q) * C + c] = (int32_t)runv;
                 runv += v;
             }
-        if (tid == 0) a.totals[c] = total;
+        // per-loop totals from the masks (the records may have run out of room)
+        if (tid == 0) a.totals[c] = c < 2 ? total : (int64_t)__ldcg(a.ctl + kCtlWords + (c - 2));
         __syncthreads();                                        // scan_w is rewritten
     }
-    grid_sync(a.ctl, 2u * (unsigned)G, err);
+    grid_sync(a.ctl, 3u * (unsigned)G, err);
 
     // ---- phase 2: survivors, slab entries, copies -------------------------------------
     if (warp == 0) {
@@ -615,11 +962,24 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_kernel(const MatterA
     __syncthreads();
     {
         const uint64_t last = l2_policy_last_use();
-        const int64_t surv_k = __ldcg(a.cta_pre + k * C);
-        int* segrel = reinterpret_cast<int*>(dyn);              // [kChunkSegs][kSegRow]
-        int64_t rem_run = 0;                                    // removed atoms of the CTA's earlier chunks
-        for (int64_t c0 = seg_lo; c0 < seg_hi; c0 += kChunkSegs) {
-            const int cn = (int)(seg_hi - c0 < kChunkSegs ? seg_hi - c0 : kChunkSegs);
+        int64_t* wrun = reinterpret_cast<int64_t*>(wq_raw) + warp * kSegRow;   // this warp's next entry per loop
+        uint64_t* smask = reinterpret_cast<uint64_t*>(dyn) + warp * (2 * kSegAtoms);
+        uint64_t* ssides = smask + kSegAtoms;
+        for (int c = lane; c < 2 * nl; c += 32) {
+            int64_t v = run[c];
+            for (int w = 0; w < warp; ++w) v += wcnt[w][c];
+            wrun[c] = v;
+        }
+        // survivors before this warp's first segment (earlier warps' segments are full)
+        int64_t surv = __ldcg(a.cta_pre + k * C);
+        for (int w = 0; w < warp; ++w) {
+            const int64_t lo_w = seg_lo + nseg * w / kMatterWarps, hi_w = seg_lo + nseg * (w + 1) / kMatterWarps;
+            surv += (hi_w - lo_w) * kSegAtoms - wrem[w];
+        }
+        __syncwarp();
+        int64_t rem_run = 0;                                    // removed atoms of the warp's earlier batches
+        for (int64_t c0 = wlo; c0 < whi; c0 += 32) {
+            const int cn = (int)(whi - c0 < 32 ? whi - c0 : 32);
             const int v_rem = lane < cn ? __ldcg(a.seg_removed + c0 + lane) : 0;
             const int v_mem = lane < cn ? __ldcg(a.seg_members + c0 + lane) : 0;
             const int v_off = lane < cn ? __ldcg(a.seg_off + c0 + lane) : 0;
@@ -629,117 +989,17 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_kernel(const MatterA
                 if (lane >= o) incl += y;
             }
             const int ex_rem = incl - v_rem;
-            const int chunk_rem = __shfl_sync(0xffffffffu, incl, 31);
-            const bool any_mem = __ballot_sync(0xffffffffu, v_mem > 0) != 0;   // the same in every warp
-            const int64_t base = surv_k + (c0 - seg_lo) * kSegAtoms - rem_run; // survivors before the chunk
+            const int64_t base = surv + (c0 - wlo) * kSegAtoms - rem_run;      // survivors before the batch
 #pragma unroll 1
-            for (int rr = 0; rr < kChunkSegs / kMatterWarps; ++rr) {
-                const int j = rr * kMatterWarps + warp;
-                if (j >= cn) break;
+            for (int j = 0; j < cn; ++j) {
                 const int64_t sbj = base + (int64_t)j * kSegAtoms - __shfl_sync(0xffffffffu, ex_rem, j);
-                copy_segment(a, c0 + j, sbj, __shfl_sync(0xffffffffu, v_rem, j), __shfl_sync(0xffffffffu, v_mem, j),
-                             __shfl_sync(0xffffffffu, v_off, j), last, lane);
+                const int m = __shfl_sync(0xffffffffu, v_mem, j), off = __shfl_sync(0xffffffffu, v_off, j);
+                if (m > 0 && (int64_t)off + m <= a.member_cap)
+                    copy_members(a, sh, vac, c0 + j, sbj, a.members + off, m, smask, ssides, wrun, last, lane);
+                else
+                    copy_plain(a, c0 + j, sbj, last, lane);
             }
-            if (any_mem) {
-                // per-loop slab and kept-copy counts of each segment of the chunk
-#pragma unroll 1
-                for (int rr = 0; rr < kChunkSegs / kMatterWarps; ++rr) {
-                    const int j = rr * kMatterWarps + warp;
-                    for (int c = lane; c < 2 * nl; c += 32) segrel[j * kSegRow + c] = 0;
-                    __syncwarp();
-                    const int m = __shfl_sync(0xffffffffu, v_mem, j), off = __shfl_sync(0xffffffffu, v_off, j);
-                    if (j < cn && m > 0 && (int64_t)off + m <= a.member_cap) {
-                        const MemberRec* rec = a.members + off;
-                        for (uint64_t u = segment_union(rec, m, lane); u; u &= u - 1) {
-                            const int l = __ffsll((long long)u) - 1;
-                            const bool inter = sh[l].type == DISCO_MATTER_INTERSTITIAL;
-                            int cin = 0, ck = 0;
-                            for (int e0 = 0; e0 < m; e0 += 32) {
-                                const int e = e0 + lane;
-                                bool in = false, kp = false;
-                                if (e < m) {
-                                    in = (__ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].mask)) >> l) & 1ull;
-                                    kp = in && inter && !__ldcg(&rec[e].removed);
-                                }
-                                cin += __popc(__ballot_sync(0xffffffffu, in));
-                                ck += __popc(__ballot_sync(0xffffffffu, kp));
-                            }
-                            if (lane == 0) { segrel[j * kSegRow + l] = cin; segrel[j * kSegRow + nl + l] = ck; }
-                        }
-                    }
-                }
-                __syncthreads();
-                // exclusive prefixes over the chunk's segments, per category
-                for (int c = warp; c < 2 * nl; c += kMatterWarps) {
-                    const int v = segrel[lane * kSegRow + c];
-                    int p = v;
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int y = __shfl_up_sync(0xffffffffu, p, o);
-                        if (lane >= o) p += y;
-                    }
-                    segrel[lane * kSegRow + c] = p - v;
-                    if (lane == 31) ctot[c] = p;
-                }
-                __syncthreads();
-                // slab entries and copies, ascending atom order within each loop
-#pragma unroll 1
-                for (int rr = 0; rr < kChunkSegs / kMatterWarps; ++rr) {
-                    const int j = rr * kMatterWarps + warp;
-                    const int m = __shfl_sync(0xffffffffu, v_mem, j), off = __shfl_sync(0xffffffffu, v_off, j);
-                    const int exr = __shfl_sync(0xffffffffu, ex_rem, j);
-                    if (j < cn && m > 0 && (int64_t)off + m <= a.member_cap) {
-                        const MemberRec* rec = a.members + off;
-                        const int64_t i0 = (c0 + j) * kSegAtoms;
-                        const int64_t sbj = base + (int64_t)j * kSegAtoms - exr;
-                        for (uint64_t u = segment_union(rec, m, lane); u; u &= u - 1) {
-                            const int l = __ffsll((long long)u) - 1;
-                            const bool inter = sh[l].type == DISCO_MATTER_INTERSTITIAL;
-                            int64_t qs = run[l] + segrel[j * kSegRow + l];
-                            int64_t qc = run[nl + l] + segrel[j * kSegRow + nl + l];
-                            int rem_before = 0;
-                            for (int e0 = 0; e0 < m; e0 += 32) {
-                                const int e = e0 + lane;
-                                MemberRec r;
-                                r.atom = 0; r.removed = 0; r.mask = 0; r.sides = 0;
-                                if (e < m) {
-                                    r.atom = __ldcg(&rec[e].atom);
-                                    r.removed = __ldcg(&rec[e].removed);
-                                    r.mask = __ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].mask));
-                                    r.sides = __ldcg(reinterpret_cast<const unsigned long long*>(&rec[e].sides));
-                                }
-                                const bool in = (r.mask >> l) & 1ull;
-                                const bool kp = in && inter && !r.removed;
-                                const unsigned bi = __ballot_sync(0xffffffffu, in);
-                                const unsigned bk = __ballot_sync(0xffffffffu, kp);
-                                const unsigned br = __ballot_sync(0xffffffffu, e < m && r.removed);
-                                const bool pos = (r.sides >> l) & 1ull;
-                                if (in) {
-                                    const int64_t q = qs + __popc(bi & ltm);
-                                    if (q >= 0 && q < a.slab_cap) { a.slab_atoms[q] = r.atom; a.slab_side[q] = pos ? 1 : -1; }
-                                }
-                                if (kp) {
-                                    const int64_t q = qc + __popc(bk & ltm);
-                                    if (q >= 0 && q < a.copy_cap) {
-                                        const disco_slab_loop& g = a.loops[l].L;
-                                        const double* shf = pos ? g.shift_pos : g.shift_neg;
-                                        disco_copy cp;
-                                        cp.atom = (int32_t)(sbj + (r.atom - i0) - (rem_before + __popc(br & ltm)));
-                                        cp.reserved = 0;
-                                        cp.shift[0] = shf[0]; cp.shift[1] = shf[1]; cp.shift[2] = shf[2];
-                                        a.copies[q] = cp;
-                                    }
-                                }
-                                qs += __popc(bi);
-                                qc += __popc(bk);
-                                rem_before += __popc(br);
-                            }
-                        }
-                    }
-                }
-                __syncthreads();                                // segrel and run are rewritten
-                for (int c = tid; c < 2 * nl; c += kMatterThreads) run[c] += ctot[c];
-            }
-            rem_run += chunk_rem;
+            rem_run += __shfl_sync(0xffffffffu, incl, 31);
         }
     }
 
@@ -749,12 +1009,14 @@ __global__ void __launch_bounds__(kMatterThreads, 4) matter_kernel(const MatterA
         const unsigned done = atomicAdd(a.ctl + 1, 1u);
         if (done == (unsigned)G - 1u) {
             a.totals[C] = atomicExch(err, 0);
+            for (int c = 0; c < 2 * nl; ++c) atomicExch(a.ctl + kCtlWords + c, 0u);
             atomicExch(a.ctl + 0, 0u);
             atomicExch(a.ctl + 2, 0u);
             atomicExch(a.ctl + 1, 0u);
         }
     }
 }
+
 // Code/main.cpp:733-743 + 797-818: copies appended with u(src) + shift, then
 // r = x + u folded once into [-L/2, L/2] and shifted by +L/2.
 __global__ void finalize_kernel(const double* __restrict__ x, const double* __restrict__ y,
@@ -880,6 +1142,10 @@ int slab_loop_record(const disco_slab_loop& g, const double box[3], disco_slab_i
     h.bound = frame ? (rho * std::sqrt(1.0 + std::fabs(c)) + smax) * (1.0 + 1e-9) + 1e-6 +
                       1e-9 * (box[0] + box[1] + box[2])
                     : HUGE_VAL;
+    {
+        const float bf = (float)h.bound;               // rounded up to the next float
+        h.boundf = std::isfinite(bf) && (double)bf < h.bound ? std::nextafter(bf, INFINITY) : bf;
+    }
     active = true;
     return DISCO_OK;
 }
@@ -967,8 +1233,9 @@ int stage_loops(const disco_slab_loop* loops, int nloops, const double box[3], d
 }
 
 // Bytes of the control words (barrier arrivals, exits, member records taken,
-// error word); the last CTA of every completed call leaves them at zero.
-constexpr size_t kCtlBytes = 16;
+// error word, per-loop totals); the last CTA of every completed call leaves
+// them at zero.
+constexpr size_t kCtlBytes = (disco::kCtlWords + 2 * disco::kMaxSlabLoops) * sizeof(unsigned int);
 
 // CTAs of the cooperative launch on the current device: resident CTAs per SM
 // times the SM count, at most kMaxGrid (cached per device; no allocation).
@@ -992,6 +1259,17 @@ int matter_grid_max(int& out)
     out = std::min(per_sm * sms, disco::kMaxGrid);
     if (dev >= 0 && dev < 64) cached[dev] = out;
     return DISCO_OK;
+}
+
+// Whether the positions and the outputs take 16-byte accesses.
+void set_vec_flags(disco::MatterArgs& a)
+{
+    const uintptr_t in = reinterpret_cast<uintptr_t>(a.x) | reinterpret_cast<uintptr_t>(a.y) |
+                         reinterpret_cast<uintptr_t>(a.z);
+    const uintptr_t out = reinterpret_cast<uintptr_t>(a.xo) | reinterpret_cast<uintptr_t>(a.yo) |
+                          reinterpret_cast<uintptr_t>(a.zo);
+    a.vec_in = (in & 15) == 0;
+    a.vec_out = (out & 15) == 0 && (reinterpret_cast<uintptr_t>(a.new_index) & 7) == 0;
 }
 
 // Segments and CTAs of a call on n atoms.
@@ -1133,10 +1411,11 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
 
     DevBuf dxyz, dout, didx, dloops, dctl, dseg, dcta, dmem, dtot, dslab, dside, dcop;
     const size_t nb = (size_t)n * sizeof(double);
+    const int64_t ns = (n + 1) & ~int64_t(1);           // array stride: every array 16-byte aligned
     cudaError_t e = cudaSuccess;
     if (n > 0) {
-        e = cudaMalloc(&dxyz.p, 3 * nb);
-        if (e == cudaSuccess) e = cudaMalloc(&dout.p, 3 * nb);
+        e = cudaMalloc(&dxyz.p, 3 * (size_t)ns * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&dout.p, 3 * (size_t)ns * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&didx.p, (size_t)n * sizeof(int32_t));
     }
     if (e == cudaSuccess) e = cudaMalloc(&dloops.p, sizeof(LoopStage));
@@ -1151,8 +1430,8 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
     if (e != cudaSuccess) return cfail(e, "prismatic allocation");
     if (n > 0) {
         e = cudaMemcpy(dxyz.as<double>(), x, nb, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(dxyz.as<double>() + n, y, nb, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(dxyz.as<double>() + 2 * n, z, nb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(dxyz.as<double>() + ns, y, nb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(dxyz.as<double>() + 2 * ns, z, nb, cudaMemcpyHostToDevice);
     }
     if (e != cudaSuccess) return cfail(e, "prismatic upload");
     st = stage_loops(loops, nloops, box, info, act_index, nl, dloops.as<unsigned char>(), nullptr);
@@ -1160,13 +1439,14 @@ int disco_b200_prismatic(const double* x, const double* y, const double* z, int6
 
     MatterArgs a;
     std::memset(&a, 0, sizeof(a));
-    a.x = dxyz.as<double>(); a.y = a.x + n; a.z = a.x + 2 * n;
+    a.x = dxyz.as<double>(); a.y = a.x + ns; a.z = a.x + 2 * ns;
     a.n = n;
     a.Lx = box[0]; a.Ly = box[1]; a.Lz = box[2];
     a.iLx = (float)(1.0 / box[0]); a.iLy = (float)(1.0 / box[1]); a.iLz = (float)(1.0 / box[2]);
     a.idLx = 1.0 / box[0]; a.idLy = 1.0 / box[1]; a.idLz = 1.0 / box[2];
-    a.xo = dout.as<double>(); a.yo = a.xo + n; a.zo = a.xo + 2 * n;
+    a.xo = dout.as<double>(); a.yo = a.xo + ns; a.zo = a.xo + 2 * ns;
     a.new_index = didx.as<int32_t>();
+    set_vec_flags(a);
     a.slab_atoms = dslab.as<int32_t>();
     a.slab_side = dside.as<int8_t>();
     a.slab_cap = slab_capacity;
@@ -1427,6 +1707,7 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
     a.idLx = 1.0 / box[0]; a.idLy = 1.0 / box[1]; a.idLz = 1.0 / box[2];
     a.xo = x_out; a.yo = y_out; a.zo = z_out;
     a.new_index = new_index;
+    set_vec_flags(a);
     a.slab_atoms = slab_atoms;
     a.slab_side = slab_side;
     a.slab_cap = slab_capacity;

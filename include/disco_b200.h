@@ -401,9 +401,10 @@ typedef struct {
  * atoms dropped.  counts = {survivors, slab entries, copies}; when a capacity
  * is too small the call returns DISCO_ELIMIT with counts holding the sizes
  * needed.  Selection is bit-exact with the reference's FP64 predicate.  On the
- * device: one pass over the atoms (each atom's slab mask computed once,
- * survivors compacted in order by decoupled look-back) and a short pass
- * writing the slab entries and copies from the slab atoms' records. */
+ * device: one cooperative kernel (each atom's slab mask computed once, counts
+ * per CTA, grid barriers around a scan of those counts, then the ordered
+ * writes of survivors, slab entries and copies).  Output arrays must not
+ * overlap the inputs. */
 int disco_b200_prismatic(const double *x, const double *y, const double *z, int64_t n,
                          const disco_slab_loop *loops, int32_t nloops, const double box[3],
                          double *x_out, double *y_out, double *z_out, int32_t *new_index,

@@ -170,7 +170,9 @@ constexpr int kSegRow = 2 * kMaxSlabLoops;                     // per-loop slab 
 constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // categories counted per CTA
 constexpr int kWarpQueue = 512;                                // exact tests queued per warp
 constexpr int kMaxGrid = 8 * 148;                              // CTAs of one call at most
-constexpr int kCtlWords = 4;                                   // control words before the per-loop totals
+constexpr int kCtlWords = 8;                                   // control words before the per-loop totals
+constexpr int kGrab = 4;                                       // segments per ticket of the first phase
+constexpr int kFlushAt = 32;                                   // queued exact tests that start a flush
 // dynamic shared memory: per warp the masks and sides of one segment
 constexpr size_t kMatterSmem = kMatterWarps * 2 * kSegAtoms * sizeof(uint64_t);
 
@@ -192,8 +194,8 @@ struct MatterArgs {
     int32_t* cta_tot;             // [G][C] counts per CTA
     int32_t* cta_pre;             // [G][C] exclusive prefixes over the CTAs
     unsigned int* ctl;            // [kCtlWords] barrier arrivals, exits, member records taken, error
-                                  // word, then [2 nl] per-loop slab and kept-copy totals; zero at
-                                  // entry, left zero by the last CTA to leave
+                                  // word, segment ticket, then [2 nl] per-loop slab and kept-copy
+                                  // totals; zero at entry, left zero by the last CTA to leave
     MemberRec* members;
     int64_t member_cap;
     double *xo, *yo, *zo;
@@ -278,34 +280,6 @@ __device__ __forceinline__ void grid_sync(unsigned* arrive, unsigned target, int
     __syncthreads();
 }
 
-// Cheap pre-test in FP32: true only if the atom's t is outside [tLo, tHi) by
-// more than `margin` planes.  With the atom and the centre within 2 L of the
-// origin and rounded to FP32, and the nearest image unambiguous (r/L + 1/2 at
-// least 1e-5 from an integer and |r/L| < 2; else it returns false), the FP32
-// t differs from the exactly rounded t of slab_member by less than
-// 1.5e-6 (Lx + Ly + Lz) / d + 1e-6 planes; the margin is
-// 1e-5 (Lx + Ly + Lz) / d + 1e-3.  So it never rejects a member: the exact
-// test decides every atom it passes, and atom sets stay bit-exact.
-__device__ __forceinline__ bool clearly_outside(const SlabHead& S, const float (&p)[3], const float (&L)[3],
-                                                const float (&iL)[3])
-{
-    float s = 0.0f;
-    bool sure = true;                     // branch-free, so that loops interleave
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float r = p[k] - S.cf[k];
-        const float q = r * iL[k];
-        const float h = q + 0.5f;
-        const float f = floorf(h);
-        const float fr = h - f;
-        sure = sure && fabsf(q) < 2.0f && fr >= 1e-5f && fr <= 1.0f - 1e-5f &&
-               fabsf(p[k]) < 2.0f * L[k] && fabsf(S.cf[k]) < 2.0f * L[k];
-        s = fmaf(S.nf[k], fmaf(-L[k], f, r), s);
-    }
-    const float t = s * S.inv_df;
-    return sure && (t < S.tlo - S.margin || t >= S.thi + S.margin);
-}
-
 // Smallest |p - c - m L| over p in [lo, hi] and integers m, in FP32 for the
 // culling: lo, hi are the FP32 roundings of a segment's extreme coordinates,
 // c and L those of the loop centre and the box.  Every rounding is covered by
@@ -324,18 +298,77 @@ __device__ __forceinline__ float periodic_gap_f(float lo, float hi, float c, flo
     return fmaxf(0.0f, d - (1e-5f * (fabsf(a) + fabsf(b) + L) + 1e-3f));
 }
 
-// The loops among `cand` (loops whose slab can reach the atom's segment) that
-// the FP32 pre-test cannot exclude for the atom at p (its position rounded to
-// FP32): its exact-test candidates.
-__device__ __forceinline__ uint64_t pretest(const SlabHead* sh, uint64_t cand, const float (&p)[3],
-                                            const float (&L)[3], const float (&iL)[3])
+// The FP32 pre-test of the lane's four atoms of a segment (f*[q], their
+// positions rounded to FP32) against the loops in `cand` (loops whose slab can
+// reach the segment): per atom the loops it cannot exclude, its exact-test
+// candidates.  A loop is excluded only if the atom's t is outside [tLo, tHi)
+// by more than `margin` planes.  With the atom and the centre within 2 L of
+// the origin and rounded to FP32, and the nearest image unambiguous (r/L + 1/2
+// at least 1e-5 from an integer and |r/L| < 2; else the loop stays a
+// candidate), the FP32 t differs from the exactly rounded t of slab_member by
+// less than 1.5e-6 (Lx + Ly + Lz) / d + 1e-6 planes; the margin is
+// 1e-5 (Lx + Ly + Lz) / d + 1e-3.  So it never rejects a member: the exact
+// test decides every atom it passes, and atom sets stay bit-exact.
+__device__ __forceinline__ void pretest_segment(const SlabHead* sh, uint64_t cand, const float (&fx)[kSegRounds],
+                                                const float (&fy)[kSegRounds], const float (&fz)[kSegRounds],
+                                                const bool (&valid)[kSegRounds], const float (&L)[3],
+                                                const float (&iL)[3], uint64_t (&out)[kSegRounds])
 {
-    uint64_t c2 = 0;
+    bool pin[kSegRounds];
+#pragma unroll
+    for (int q = 0; q < kSegRounds; ++q) {
+        pin[q] = fabsf(fx[q]) < 2.0f * L[0] && fabsf(fy[q]) < 2.0f * L[1] && fabsf(fz[q]) < 2.0f * L[2];
+        out[q] = 0ull;
+    }
     for (uint64_t c = cand; c; c &= c - 1) {
         const int l = __ffsll((long long)c) - 1;
-        if (!clearly_outside(sh[l], p, L, iL)) c2 |= 1ull << l;
+        const SlabHead& S = sh[l];
+        const float cx = S.cf[0], cy = S.cf[1], cz = S.cf[2];
+        const float nx = S.nf[0], ny = S.nf[1], nz = S.nf[2];
+        const float tlo = S.tlo - S.margin, thi = S.thi + S.margin, idf = S.inv_df;
+        const bool cin = fabsf(cx) < 2.0f * L[0] && fabsf(cy) < 2.0f * L[1] && fabsf(cz) < 2.0f * L[2];
+#pragma unroll
+        for (int q = 0; q < kSegRounds; ++q) {
+            const float p[3] = { fx[q], fy[q], fz[q] };
+            const float cc[3] = { cx, cy, cz }, nn[3] = { nx, ny, nz };
+            float s = 0.0f;
+            bool sure = pin[q] && cin;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float r = p[k] - cc[k];
+                const float qd = r * iL[k];
+                const float h = qd + 0.5f;
+                const float f = floorf(h);
+                const float fr = h - f;
+                sure = sure && fabsf(qd) < 2.0f && fr >= 1e-5f && fr <= 1.0f - 1e-5f;
+                s = fmaf(nn[k], fmaf(-L[k], f, r), s);
+            }
+            const float t = s * idf;
+            const bool outside = sure && (t < tlo || t >= thi);
+            if (valid[q] && !outside) out[q] |= 1ull << l;
+        }
     }
-    return c2;
+}
+
+// Warp-wide minimum / maximum of a float through the integer reduction unit:
+// the bit pattern, its magnitude bits flipped for negative values, orders as a
+// signed integer exactly as the floats order (NaN aside, which no member has).
+__device__ __forceinline__ int float_order(float f)
+{
+    const int i = __float_as_int(f);
+    return i ^ ((i >> 31) & 0x7fffffff);
+}
+
+__device__ __forceinline__ float order_float(int i) { return __int_as_float(i ^ ((i >> 31) & 0x7fffffff)); }
+
+__device__ __forceinline__ float warp_min_f(float v)
+{
+    return order_float(__reduce_min_sync(0xffffffffu, float_order(v)));
+}
+
+__device__ __forceinline__ float warp_max_f(float v)
+{
+    return order_float(__reduce_max_sync(0xffffffffu, float_order(v)));
 }
 
 // Streaming layout of a segment: lane t holds the atoms 64 (q / 2) + 2 t + q % 2,
@@ -667,21 +700,30 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
         const double* pf_base = lane < 8 ? a.x : lane < 16 ? a.y : a.z;
         const float Lf[3] = { (float)a.Lx, (float)a.Ly, (float)a.Lz };
         const float iLf[3] = { a.iLx, a.iLy, a.iLz };
-        const int64_t W = (int64_t)G * kMatterWarps, gw = k * kMatterWarps + warp;
-        const int64_t nj = gw < a.S ? (a.S - 1 - gw) / W + 1 : 0;
-        for (int64_t j0 = 0; j0 < nj; j0 += kGroupSegs) {
-            const int64_t j1 = nj - j0 < kGroupSegs ? nj : j0 + kGroupSegs;
+        // segments in chunks of kGrab from the call's ticket, the next chunk
+        // taken one ahead: warps that meet slabs take fewer segments
+        unsigned tk = 0;
+        if (lane == 0) tk = atomicAdd(a.ctl + 4, (unsigned)kGrab);
+        int64_t cur = __shfl_sync(0xffffffffu, tk, 0);
+        if (lane == 0) tk = atomicAdd(a.ctl + 4, (unsigned)kGrab);
+        int64_t nxt = __shfl_sync(0xffffffffu, tk, 0);
+        int64_t s = cur;                                        // the next segment
+        while (true) {
             int nq = 0, nlst = 0;
-            for (int64_t j = j0; j < j1; ++j) {
-                const int64_t s = gw + j * W;
-                const int64_t i0 = s * kSegAtoms;
-                if (lane < 24 && j + 2 < nj) {
-                    const int64_t pi = (s + 2 * W) * kSegAtoms + (lane & 7) * 16;
-                    if (pi < a.n) prefetch_l2_keep(pf_base + pi);
+            while (nlst < kGroupSegs && nq < kFlushAt && s < a.S) {
+                const int64_t cend = cur + kGrab < a.S ? cur + kGrab : a.S;
+                {
+                    const int64_t p2 = s + 2 < cend ? s + 2 : nxt + (s + 2 - cend);   // two segments ahead
+                    if (lane < 24 && p2 < a.S) {
+                        const int64_t pi = p2 * kSegAtoms + (lane & 7) * 16;
+                        if (pi < a.n) prefetch_l2_keep(pf_base + pi);
+                    }
                 }
+                const int64_t i0 = s * kSegAtoms;
                 // the segment's positions rounded to FP32 (slot_of layout); an
                 // atom past n repeats the segment's first atom
                 float fx[kSegRounds], fy[kSegRounds], fz[kSegRounds];
+                bool valid[kSegRounds];
                 if (a.vec_in && i0 + kSegAtoms <= a.n) {
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
@@ -694,11 +736,14 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
                         fy[2 * h] = (float)y0; fy[2 * h + 1] = (float)y1;
                         fz[2 * h] = (float)z0; fz[2 * h + 1] = (float)z1;
                     }
+#pragma unroll
+                    for (int q = 0; q < kSegRounds; ++q) valid[q] = true;
                 } else {
 #pragma unroll
                     for (int q = 0; q < kSegRounds; ++q) {
                         int64_t i = i0 + slot_of(q, lane);
-                        if (i >= a.n) i = i0;
+                        valid[q] = i < a.n;
+                        if (!valid[q]) i = i0;
                         fx[q] = (float)ld_hint(a.x + i, keep);
                         fy[q] = (float)ld_hint(a.y + i, keep);
                         fz[q] = (float)ld_hint(a.z + i, keep);
@@ -714,12 +759,10 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
                                     fmaxf(fmaxf(fy[0], fy[1]), fmaxf(fy[2], fy[3])),
                                     fmaxf(fmaxf(fz[0], fz[1]), fmaxf(fz[2], fz[3])) };
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-                            hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
-                        }
+                    for (int d = 0; d < 3; ++d) {
+                        lo[d] = warp_min_f(lo[d]);
+                        hi[d] = warp_max_f(hi[d]);
+                    }
                     for (int half = 0; half * 32 < nl; ++half) {
                         const int l = lane + 32 * half;
                         bool reach = false;
@@ -738,13 +781,10 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
                 if (wmask) {
                     // the FP32 pre-test per atom: its exact-test candidates
                     uint64_t cand[kSegRounds];
+                    pretest_segment(sh, wmask, fx, fy, fz, valid, Lf, iLf, cand);
                     int cnt = 0;
 #pragma unroll
-                    for (int q = 0; q < kSegRounds; ++q) {
-                        const float p[3] = { fx[q], fy[q], fz[q] };
-                        cand[q] = i0 + slot_of(q, lane) < a.n ? pretest(sh, wmask, p, Lf, iLf) : 0ull;
-                        cnt += __popcll(cand[q]);
-                    }
+                    for (int q = 0; q < kSegRounds; ++q) cnt += __popcll(cand[q]);
                     int pre = cnt;
                     for (int o = 1; o < 32; o <<= 1) {
                         const int y = __shfl_up_sync(0xffffffffu, pre, o);
@@ -753,15 +793,15 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
                     const int T = __shfl_sync(0xffffffffu, pre, 31);
                     pre -= cnt;
                     if (T > 0 && nq + T <= kWarpQueue) {
-                        // queued: (loop, slot, segment of the group), tested at the flush
+                        // queued: (loop, slot, list entry), tested at the flush
                         int q = nq + pre;
 #pragma unroll
                         for (int r = 0; r < kSegRounds; ++r)
                             for (uint64_t c = cand[r]; c; c &= c - 1)
                                 wq[q++] = (uint32_t)(__ffsll((long long)c) - 1) | ((uint32_t)slot_of(r, lane) << 6) |
-                                          ((uint32_t)(j - j0) << 13);
+                                          ((uint32_t)nlst << 13);
                         if (lane == 0) {
-                            wl_seg[warp][nlst] = (int)(j - j0);
+                            wl_seg[warp][nlst] = (int)s;
                             wl_q[warp][nlst] = nq | (T << 16);
                         }
                         nq += T;
@@ -777,81 +817,91 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
                     }
                 }
                 if (!listed && lane == 0) { a.seg_removed[s] = rc; a.seg_members[s] = mc; a.seg_off[s] = off; }
-            }
-            if (nq == 0) continue;
-            // flush: the exact tests of the queue spread over the lanes, the
-            // result in bits 29 (member) and 30 (positive side) of each entry
-            __syncwarp();
-            for (int q = lane; q < nq; q += 32) {
-                const uint32_t e = wq[q];
-                const int l = e & 63, slot = (e >> 6) & 127;
-                const int64_t i = (gw + (j0 + (e >> 13)) * W) * kSegAtoms + slot;
-                bool ps = false;
-                const bool in = slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx, a.idLy,
-                                            a.idLz, ps);
-                wq[q] = e | (in ? 1u << 29 : 0u) | (ps ? 1u << 30 : 0u);
-            }
-            __syncwarp();
-            // member and removed counts per listed segment, then one block of records
-            int tot = 0;
-            for (int jj = 0; jj < nlst; ++jj) {
-                const int qo = wl_q[warp][jj] & 0xffff, qn = wl_q[warp][jj] >> 16;
-                unsigned mb[kSegRounds], rbm[kSegRounds];
-#pragma unroll
-                for (int r = 0; r < kSegRounds; ++r) { mb[r] = 0u; rbm[r] = 0u; }
-                for (int q0 = 0; q0 < qn; q0 += 32) {
-                    unsigned slot = 0xffffffffu;
-                    bool rmv = false;
-                    if (q0 + lane < qn) {
-                        const uint32_t e = wq[qo + q0 + lane];
-                        if (e & (1u << 29)) {
-                            slot = (e >> 6) & 127;
-                            rmv = (vac >> (e & 63)) & 1ull;
-                        }
-                    }
-#pragma unroll
-                    for (int r = 0; r < kSegRounds; ++r) {
-                        const unsigned bit = (slot >> 5) == (unsigned)r ? 1u << (slot & 31u) : 0u;
-                        mb[r] |= __reduce_or_sync(0xffffffffu, bit);
-                        rbm[r] |= __reduce_or_sync(0xffffffffu, rmv ? bit : 0u);
+                if (++s >= cend) {                              // the next chunk
+                    cur = nxt;
+                    s = cur;
+                    if (cur < a.S) {
+                        if (lane == 0) tk = atomicAdd(a.ctl + 4, (unsigned)kGrab);
+                        nxt = __shfl_sync(0xffffffffu, tk, 0);
                     }
                 }
-                int m = 0, rm = 0;
-#pragma unroll
-                for (int r = 0; r < kSegRounds; ++r) { m += __popc(mb[r]); rm += __popc(rbm[r]); }
-                if (lane == 0) wl_mr[warp][jj] = m | (rm << 16);
-                tot += m;
             }
-            int base = 0;
-            if (lane == 0 && tot > 0) base = (int)atomicAdd(a.ctl + 2, (unsigned)tot);
-            base = __shfl_sync(0xffffffffu, base, 0);
-            __syncwarp();
-            for (int jj = 0; jj < nlst; ++jj) {
-                const int64_t s = gw + (j0 + wl_seg[warp][jj]) * W;
-                const int m = wl_mr[warp][jj] & 0xffff, rm = wl_mr[warp][jj] >> 16;
-                if (m > 0) {
+            if (nq > 0) {
+                // flush: the exact tests of the queue spread over the lanes, the
+                // result in bits 29 (member) and 30 (positive side) of each entry
+                __syncwarp();
+                for (int q = lane; q < nq; q += 32) {
+                    const uint32_t e = wq[q];
+                    const int l = e & 63, slot = (e >> 6) & 127;
+                    const int64_t i = (int64_t)wl_seg[warp][(e >> 13) & 31] * kSegAtoms + slot;
+                    bool ps = false;
+                    const bool in = slab_member(a.loops[l], a.x[i], a.y[i], a.z[i], a.Lx, a.Ly, a.Lz, a.idLx,
+                                                a.idLy, a.idLz, ps);
+                    wq[q] = e | (in ? 1u << 29 : 0u) | (ps ? 1u << 30 : 0u);
+                }
+                __syncwarp();
+                // member and removed counts per listed segment, then one block of records
+                int tot = 0;
+                for (int jj = 0; jj < nlst; ++jj) {
                     const int qo = wl_q[warp][jj] & 0xffff, qn = wl_q[warp][jj] >> 16;
+                    unsigned mb[kSegRounds], rbm[kSegRounds];
 #pragma unroll
-                    for (int r = 0; r < kSegRounds; ++r) { smask[r * 32 + lane] = 0; ssides[r * 32 + lane] = 0; }
-                    __syncwarp();
-                    for (int q = lane; q < qn; q += 32) {
-                        const uint32_t e = wq[qo + q];
-                        if (e & (1u << 29)) {
-                            const int slot = (e >> 6) & 127;
-                            atomicOr(reinterpret_cast<unsigned long long*>(&smask[slot]), 1ull << (e & 63));
-                            if (e & (1u << 30))
-                                atomicOr(reinterpret_cast<unsigned long long*>(&ssides[slot]), 1ull << (e & 63));
+                    for (int r = 0; r < kSegRounds; ++r) { mb[r] = 0u; rbm[r] = 0u; }
+                    for (int q0 = 0; q0 < qn; q0 += 32) {
+                        unsigned slot = 0xffffffffu;
+                        bool rmv = false;
+                        if (q0 + lane < qn) {
+                            const uint32_t e = wq[qo + q0 + lane];
+                            if (e & (1u << 29)) {
+                                slot = (e >> 6) & 127;
+                                rmv = (vac >> (e & 63)) & 1ull;
+                            }
+                        }
+#pragma unroll
+                        for (int r = 0; r < kSegRounds; ++r) {
+                            const unsigned bit = (slot >> 5) == (unsigned)r ? 1u << (slot & 31u) : 0u;
+                            mb[r] |= __reduce_or_sync(0xffffffffu, bit);
+                            rbm[r] |= __reduce_or_sync(0xffffffffu, rmv ? bit : 0u);
                         }
                     }
-                    __syncwarp();
-                    int rc2 = 0, mc2 = 0, off2 = base;
-                    aggregate_segment(a, sh, vac, s, smask, ssides, wcnt[warp], rc2, mc2, off2, lane);
-                    __syncwarp();
+                    int m = 0, rm = 0;
+#pragma unroll
+                    for (int r = 0; r < kSegRounds; ++r) { m += __popc(mb[r]); rm += __popc(rbm[r]); }
+                    if (lane == 0) wl_mr[warp][jj] = m | (rm << 16);
+                    tot += m;
                 }
-                if (lane == 0) { a.seg_removed[s] = rm; a.seg_members[s] = m; a.seg_off[s] = m > 0 ? base : 0; }
-                base += m;
+                int base = 0;
+                if (lane == 0 && tot > 0) base = (int)atomicAdd(a.ctl + 2, (unsigned)tot);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                __syncwarp();
+                for (int jj = 0; jj < nlst; ++jj) {
+                    const int64_t sj = wl_seg[warp][jj];
+                    const int m = wl_mr[warp][jj] & 0xffff, rm = wl_mr[warp][jj] >> 16;
+                    if (m > 0) {
+                        const int qo = wl_q[warp][jj] & 0xffff, qn = wl_q[warp][jj] >> 16;
+#pragma unroll
+                        for (int r = 0; r < kSegRounds; ++r) { smask[r * 32 + lane] = 0; ssides[r * 32 + lane] = 0; }
+                        __syncwarp();
+                        for (int q = lane; q < qn; q += 32) {
+                            const uint32_t e = wq[qo + q];
+                            if (e & (1u << 29)) {
+                                const int slot = (e >> 6) & 127;
+                                atomicOr(reinterpret_cast<unsigned long long*>(&smask[slot]), 1ull << (e & 63));
+                                if (e & (1u << 30))
+                                    atomicOr(reinterpret_cast<unsigned long long*>(&ssides[slot]), 1ull << (e & 63));
+                            }
+                        }
+                        __syncwarp();
+                        int rc2 = 0, mc2 = 0, off2 = base;
+                        aggregate_segment(a, sh, vac, sj, smask, ssides, wcnt[warp], rc2, mc2, off2, lane);
+                        __syncwarp();
+                    }
+                    if (lane == 0) { a.seg_removed[sj] = rm; a.seg_members[sj] = m; a.seg_off[sj] = m > 0 ? base : 0; }
+                    base += m;
+                }
+                __syncwarp();                                   // the queue and the list are rewritten
             }
-            __syncwarp();                                       // the queue is rewritten
+            if (s >= a.S) break;
         }
         // the warp's per-loop counts into the call's per-loop totals (exact
         // whether or not every member record found room)
@@ -875,12 +925,23 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
             const int v_off = lane < cn ? __ldcg(a.seg_off + c0 + lane) : 0;
             rem += __reduce_add_sync(0xffffffffu, v_rem);
             mem += __reduce_add_sync(0xffffffffu, v_mem);
-            for (unsigned b = __ballot_sync(0xffffffffu, v_mem > 0); b; b &= b - 1) {
-                const int j = __ffs(b) - 1;
-                const int m = __shfl_sync(0xffffffffu, v_mem, j), off = __shfl_sync(0xffffffffu, v_off, j);
-                if ((int64_t)off + m > a.member_cap) continue;
-                for (int e = lane; e < m; e += 32) {
-                    const MemberRec* rec = a.members + off + e;
+            // the batch's member records as one list spread over the lanes
+            const int mm = v_mem > 0 && (int64_t)v_off + v_mem <= a.member_cap ? v_mem : 0;
+            int incl = mm;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int ex = incl - mm, tot = __shfl_sync(0xffffffffu, incl, 31);
+            for (int e0 = 0; e0 < tot; e0 += 32) {
+                const int e = e0 + lane;
+                int j = 0;                                      // the last segment whose records start at or before e
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1)
+                    if (__shfl_sync(0xffffffffu, ex, j + step) <= e) j += step;
+                const int oj = __shfl_sync(0xffffffffu, v_off, j), exj = __shfl_sync(0xffffffffu, ex, j);
+                if (e < tot) {
+                    const MemberRec* rec = a.members + oj + (e - exj);
                     const uint64_t mk = __ldcg(reinterpret_cast<const unsigned long long*>(&rec->mask));
                     const bool removed = __ldcg(&rec->removed) != 0;
                     for (uint64_t u = mk; u; u &= u - 1) {
@@ -1012,6 +1073,7 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
             for (int c = 0; c < 2 * nl; ++c) atomicExch(a.ctl + kCtlWords + c, 0u);
             atomicExch(a.ctl + 0, 0u);
             atomicExch(a.ctl + 2, 0u);
+            atomicExch(a.ctl + 4, 0u);
             atomicExch(a.ctl + 1, 0u);
         }
     }

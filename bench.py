@@ -1117,10 +1117,10 @@ def run_learned(args, embedded=None):
         dist.destroy_process_group()
 
 
-def compaction_rate(lib, C, torch, stream):
+def compaction_rate(lib, C, torch, stream, cells=128):
     """The matter step alone (disco_b200_prismatic_noalloc: slab membership,
-    stable compaction, new-index map, slab entries, copies) on the largest box
-    it takes, BCC 128^3 = 4 194 304 atoms with 16 loops of the bcc_prismatic
+    stable compaction, new-index map, slab entries, copies) on a BCC box of
+    cells^3 (2 cells^3 atoms; 128: 4 194 304) with 16 loops of the bcc_prismatic
     distribution: achieved GB/s of the algorithmic bytes (52 B per atom:
     positions read once, survivors written, 4 B new index; the slab entries
     and copies add a few hundred KB) against the measured HBM peak.  Timed per
@@ -1128,7 +1128,7 @@ def compaction_rate(lib, C, torch, stream):
     device-to-host read of the totals (its only host wait)."""
     import ctypes
     from disco_b200 import workloads as W
-    w = W.bcc_prismatic(cells=128)
+    w = W.bcc_prismatic(cells=cells)
     n = w.n
     pos = torch.tensor(np.stack([w.x, w.y, w.z]), dtype=torch.float64, device="cuda")
     out = torch.empty((3, n), dtype=torch.float64, device="cuda")
@@ -1162,7 +1162,7 @@ def compaction_rate(lib, C, torch, stream):
     return {"atoms": n, "survivors": int(counts[0]), "slab_atoms": int(counts[1]), "copies": int(counts[2]),
             "ms": 1e3 * t, "atoms_per_s": n / t, "algorithmic_bytes": 52 * n, "achieved_gbs": gbs,
             "peak_gbs": peak, "frac": gbs / peak, "l2": "flushed before each timed call",
-            "traffic": traffic_from_profiles("compaction_bcc128"),
+            "traffic": traffic_from_profiles("compaction_bcc128") if cells == 128 else None,
             "traffic_what": "DRAM bytes read + written by one matter_kernel launch (ncu, profiles/compaction_bcc128.md)",
             "timed": "whole call (loop upload, matter kernel, totals read back) with CUDA events",
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk else "fallback 6650 GB/s"}
@@ -1366,9 +1366,12 @@ def run_matter(args):
     from disco_b200 import _capi as C
     torch.cuda.set_device(dist_env()[2])
     r = compaction_rate(C.cuda_lib(), C, torch, torch.cuda.current_stream())
+    big = compaction_rate(C.cuda_lib(), C, torch, torch.cuda.current_stream(), cells=189)
     print(json.dumps({"metric": "matter step atoms/s", "value": r["atoms_per_s"], "unit": "atoms/s",
                       "config": {"workload": "bcc_prismatic 128^3 (4 194 304 atoms, 16 loops)"},
-                      "compaction": r}), flush=True)
+                      "compaction": r,
+                      "compaction_13m": dict(big, workload="bcc_prismatic 189^3 (13 502 538 atoms, 16 loops)")}),
+          flush=True)
 
 
 def main():

@@ -1620,12 +1620,12 @@ int disco_b200_finalize_resident(const double* x, const double* y, const double*
 // cudaMalloc.  disco_b200_prismatic_noalloc takes device inputs and outputs
 // from the caller and keeps its scratch (loop table, control words, per-segment
 // and per-CTA counts and prefixes, member records, totals) in the file-scope
-// array below: 4 MiB
+// array below: 8 MiB
 // that every GPU loading this library holds until the process exits.
 
 namespace {
 
-constexpr int64_t kNoAllocMaxAtoms = int64_t(1) << 22;                  // 4 194 304 atoms
+constexpr int64_t kNoAllocMaxAtoms = int64_t(1) << 24;                  // 16 777 216 atoms
 constexpr int64_t kNoAllocMaxSegs = kNoAllocMaxAtoms / disco::kSegAtoms;
 constexpr int64_t kNoAllocMaxMembers = int64_t(1) << 16;                // atoms in slabs
 constexpr size_t align256c(size_t v) { return (v + 255) & ~size_t(255); }
@@ -1637,7 +1637,7 @@ constexpr size_t kNoAllocMemberOff =
     kNoAllocCtaOff + align256c(2 * (size_t)disco::kMaxGrid * disco::kMaxCats * sizeof(int32_t));
 constexpr size_t kNoAllocTotalsOff =
     kNoAllocMemberOff + align256c((size_t)kNoAllocMaxMembers * sizeof(disco::MemberRec));
-constexpr size_t kNoAllocScratchBytes = 4 * 1024 * 1024;
+constexpr size_t kNoAllocScratchBytes = 8 * 1024 * 1024;
 static_assert(kNoAllocTotalsOff + (disco::kMaxCats + 1) * sizeof(int64_t) <= kNoAllocScratchBytes,
               "no-alloc scratch layout");
 
@@ -1737,7 +1737,7 @@ int disco_b200_prismatic_noalloc(const double* x, const double* y, const double*
         return efail(DISCO_EINVAL, "null or negative argument");
     if (!(box[0] > 0.) || !(box[1] > 0.) || !(box[2] > 0.)) return efail(DISCO_EINVAL, "box lengths must be positive");
     if (n > kNoAllocMaxAtoms)
-        return efail(DISCO_ELIMIT, "disco_b200_prismatic_noalloc takes at most 4194304 atoms (its scratch array is fixed)");
+        return efail(DISCO_ELIMIT, "disco_b200_prismatic_noalloc takes at most 16777216 atoms (its scratch array is fixed)");
     int dcount = 0;
     if (cudaGetDeviceCount(&dcount) != cudaSuccess || dcount == 0) return efail(DISCO_ENODEV, "no CUDA device");
     cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -420,9 +420,9 @@ int disco_b200_prismatic(const double *x, const double *y, const double *z, int6
  * except info and counts are DEVICE pointers the caller allocated; loops,
  * box, info and counts are host memory.  Work is queued on `stream` (a
  * cudaStream_t; NULL = legacy default stream) and the call waits for it once,
- * at the end, to read the totals.  Scratch lives in a fixed 4 MiB device
+ * at the end, to read the totals.  Scratch lives in a fixed 8 MiB device
  * array inside the library (held by every GPU that loads it until the process
- * exits): at most 4 194 304 atoms, 64 prismatic loops and 65 536 atoms in
+ * exits): at most 16 777 216 atoms, 64 prismatic loops and 65 536 atoms in
  * slabs per call, DISCO_ELIMIT beyond.  The first call on a device looks up
  * that array's device address (again after a device reset gives the device a
  * new context), so make it before any stream capture.  All calls share the

@@ -77,10 +77,10 @@ def test_noalloc_rejects_sizes_beyond_its_array():
     box = (ctypes.c_double * 3)(*w.box)
     buf = torch.zeros(16, dtype=torch.float64, device="cuda")
     p = buf.data_ptr()
-    st = lib.disco_b200_prismatic_noalloc(p, p, p, (1 << 22) + 1, loops, nl, box, p, p, p, p, info,
+    st = lib.disco_b200_prismatic_noalloc(p, p, p, (1 << 24) + 1, loops, nl, box, p, p, p, p, info,
                                           p, p, 0, None, 0, counts, None)
     assert st == C.DISCO_ELIMIT
-    assert b"4194304" in lib.disco_b200_last_error()
+    assert b"16777216" in lib.disco_b200_last_error()
     # too small a slab capacity: DISCO_ELIMIT with the size needed in counts[1]
     st, counts, *_ = _noalloc(lib, torch, w, 1, 1, torch.cuda.current_stream().cuda_stream)
     assert st == C.DISCO_ELIMIT and counts[1] > 1

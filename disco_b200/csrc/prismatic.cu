@@ -173,6 +173,7 @@ constexpr int kMaxGrid = 8 * 148;                              // CTAs of one ca
 constexpr int kCtlWords = 8;                                   // control words before the per-loop totals
 constexpr int kGrab = 4;                                       // segments per ticket of the first phase
 constexpr int kFlushAt = 32;                                   // queued exact tests that start a flush
+constexpr int kSmallGrid = 64;                                 // grids scanned by one CTA
 // dynamic shared memory: per warp the masks and sides of one segment
 constexpr size_t kMatterSmem = kMatterWarps * 2 * kSegAtoms * sizeof(uint64_t);
 
@@ -967,7 +968,21 @@ __global__ void __launch_bounds__(kMatterThreads, 3) matter_kernel(const MatterA
     }
     grid_sync(a.ctl, 2u * (unsigned)G, err);
 
-    // ---- scan: CTA c takes category c, exclusive prefixes over the CTAs --------------
+    // ---- scan: exclusive prefixes over the CTAs per category.  A small grid
+    // (small boxes) is scanned by CTA 0 alone, one category per thread; a
+    // large one by CTA c for category c.
+    if (G <= kSmallGrid) {
+        if (blockIdx.x == 0)
+            for (int c = tid; c < C; c += kMatterThreads) {
+                int64_t runv = 0;
+                for (int q = 0; q < G; ++q) {
+                    const int32_t v = __ldcg(a.cta_tot + (int64_t)q * C + c);
+                    a.cta_pre[(int64_t)q * C + c] = (int32_t)runv;
+                    runv += v;
+                }
+                a.totals[c] = c < 2 ? runv : (int64_t)__ldcg(a.ctl + kCtlWords + (c - 2));
+            }
+    } else
     for (int c = blockIdx.x; c < C; c += G) {
         const int per = (G + kMatterThreads - 1) / kMatterThreads;
         const int k0 = tid * per;

@@ -57,6 +57,16 @@ def test_overlapping_slabs_many_loops(seed):
     _same(P.prismatic(x, y, z, w.slab_loops, w.box), O.prismatic(x, y, z, w.slab_loops, w.box))
 
 
+def test_overlapping_slabs_large_grid():
+    """Dense overlapping slabs on a box large enough (128 000 atoms, more than
+    64 CTAs) that the CTA counts are scanned by one CTA per category, with a
+    ragged end."""
+    w = W.bcc_prismatic(cells=40, rmin=5.0, rmax=14.0, n_inter=24, n_vac=24, seed=7)
+    k = w.n - 77
+    x, y, z = w.x[:k], w.y[:k], w.z[:k]
+    _same(P.prismatic(x, y, z, w.slab_loops, w.box), O.prismatic(x, y, z, w.slab_loops, w.box))
+
+
 def _shape_loops(a0, cells, lattice):
     """Every loop shape of the reference: circles, rounded rectangles,
     parallelograms, sharp and rounded polygons, on prismatic and mixed systems."""

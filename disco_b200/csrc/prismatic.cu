@@ -11,7 +11,7 @@
 // The step is one cooperative kernel (matter_kernel): a first phase computes
 // every atom's slab mask once (FP32 bounding-box culling per 128-atom
 // segment, an FP32 pre-test, the exact FP64 predicate for the rest, segments
-// spread round-robin over the grid's warps); after a grid barrier each CTA
+// handed to the grid's warps in chunks from a ticket); after a grid barrier each CTA
 // counts its contiguous range, after a second the CTAs' counts are scanned
 // per category, and after a third the survivors are compacted in order (x, y,
 // z and the new-index map; the positions come back from L2) and the slab
@@ -631,16 +631,16 @@ __device__ __noinline__ int3 direct_segment(const MatterArgs& a, const SlabHead*
 }
 
 // The matter step in one cooperative launch.
-//   Phase 1, masks.  The grid's warps take the 128-atom segments round-robin
-//     (warp g takes g, g + W, g + 2 W, ...), so that loops clustered in space
-//     load every SM alike.  Per segment: the positions (16-byte loads,
-//     prefetched two segments ahead, kept in L2 for phase 2) rounded to FP32
-//     for a bounding box and a per-loop cull; for the few segments a loop can
-//     reach, the FP32 pre-test per atom, its candidate (atom, loop) pairs
-//     queued per warp.  After every 32 segments the warp runs the exact FP64
-//     tests of its queue spread over its lanes, then per listed segment the
-//     masks, counts and member records (atom order, one block of records per
-//     flush).  Per segment: removed and member counts, first record; per
+//   Phase 1, masks.  The grid's warps take the 128-atom segments in chunks
+//     of four from a ticket, so that the warps whose chunks cross slabs take
+//     fewer.  Per segment: the positions (16-byte loads, prefetched two
+//     segments ahead, kept in L2 for phase 2) rounded to FP32 for a bounding
+//     box and a per-loop cull; for the few segments a loop can reach, the
+//     FP32 pre-test per atom, its candidate (atom, loop) pairs queued per
+//     warp.  Once 32 tests are queued (or 32 segments listed) the warp runs
+//     the exact FP64 tests of its queue spread over its lanes, then per listed
+//     segment the masks, counts and member records (atom order, one block of
+//     records per flush).  Per segment: removed and member counts, first record; per
 //     call: the per-loop slab and kept-copy totals.
 //   Barrier; per CTA, its counts from the per-segment results, per warp of
 //     its contiguous range; barrier; CTA c scans category c over the CTAs;

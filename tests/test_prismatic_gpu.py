@@ -67,6 +67,24 @@ def test_overlapping_slabs_large_grid():
     _same(P.prismatic(x, y, z, w.slab_loops, w.box), O.prismatic(x, y, z, w.slab_loops, w.box))
 
 
+def test_unwrapped_coordinates():
+    """Atoms moved by whole box lengths, up to 2000 L from the box, as an
+    unwrapped trajectory gives them: the minimum image decides membership
+    (Code/prismatic.cpp:31-34), the FP32 pre-test cannot vouch for such atoms
+    and hands every nearby loop to the exact test, and segments whose atoms
+    scatter over many images overflow the warp's test queue.  Atom sets and
+    the survivors' (unwrapped) positions bit-exact with the oracle."""
+    w = W.bcc_prismatic(cells=12, rmin=4.0, rmax=10.0, n_inter=6, n_vac=6, seed=11)
+    rng = np.random.default_rng(12)
+    k = rng.choice([-2000, -3, -1, 0, 0, 0, 1, 2, 2000], size=(3, w.n))
+    x = w.x + k[0] * w.box[0]
+    y = w.y + k[1] * w.box[1]
+    z = w.z + k[2] * w.box[2]
+    r = P.prismatic(x, y, z, w.slab_loops, w.box)
+    _same(r, O.prismatic(x, y, z, w.slab_loops, w.box))
+    assert len(r["slab_atoms"]) > 0
+
+
 def _shape_loops(a0, cells, lattice):
     """Every loop shape of the reference: circles, rounded rectangles,
     parallelograms, sharp and rounded polygons, on prismatic and mixed systems."""

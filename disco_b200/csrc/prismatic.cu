@@ -171,7 +171,7 @@ constexpr int kMaxCats = 2 + 2 * kMaxSlabLoops;                // categories cou
 constexpr int kWarpQueue = 512;                                // exact tests queued per warp
 constexpr int kMaxGrid = 8 * 148;                              // CTAs of one call at most
 constexpr int kCtlWords = 8;                                   // control words before the per-loop totals
-constexpr int kGrab = 4;                                       // segments per ticket of the first phase
+constexpr int kGrab = 2;                                       // segments per ticket of the first phase
 constexpr int kFlushAt = 32;                                   // queued exact tests that start a flush
 constexpr int kSmallGrid = 64;                                 // grids scanned by one CTA
 // dynamic shared memory: per warp the masks and sides of one segment
@@ -632,7 +632,7 @@ __device__ __noinline__ int3 direct_segment(const MatterArgs& a, const SlabHead*
 
 // The matter step in one cooperative launch.
 //   Phase 1, masks.  The grid's warps take the 128-atom segments in chunks
-//     of four from a ticket, so that the warps whose chunks cross slabs take
+//     of two from a ticket, so that the warps whose chunks cross slabs take
 //     fewer.  Per segment: the positions (16-byte loads, prefetched two
 //     segments ahead, kept in L2 for phase 2) rounded to FP32 for a bounding
 //     box and a per-loop cull; for the few segments a loop can reach, the

@@ -650,6 +650,7 @@ def north_star_forms(args, w, pos, u64, idx, uref):
     out["bcc_prismatic"] = {
         "value": pr["value"], "unit": "atoms/s", "ms_per_step": pr["ms_per_step"], "steps": pr["steps"],
         "config": pr["config"], "parity": pr["parity"], "compaction": pr["compaction"],
+        "compaction_13m": pr.get("compaction_13m"),
         "roofline_loopon_field": pr["roofline"], "clocks": pr["clocks"], "gpu_launches": pr["gpu_launches"]}
     return out
 

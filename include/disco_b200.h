@@ -305,8 +305,10 @@ typedef struct {
 /* Learned displacement: u += the exact field of every loop over the near images
  * max|n| < norm->image_min (opt->precision) plus the network's far shells
  * image_min <= max|n| <= norm->images, with the exact far-shell sum
- * (opt->check_precision) recomputed per loop on a random atom subsample every
- * call and replacing the network for the loops that miss the tolerances.
+ * (opt->check_precision: DISCO_FP64, or DISCO_FP32C, within about 1e-5 A of
+ * FP64 on a whole sum and twice as fast) recomputed per loop on a random atom
+ * subsample every call and replacing the network for the loops that miss the
+ * tolerances.
  * DEVICE atoms; the call returns when the work is done. */
 int disco_b200_learned_displace(disco_mlp *m, const disco_far_norm *norm, const disco_atoms *device_atoms,
                                 const disco_loop *loops, int32_t nloops, const double box[3],

@@ -1164,7 +1164,7 @@ def compaction_rate(lib, C, torch, stream, cells=128):
             "ms": 1e3 * t, "atoms_per_s": n / t, "algorithmic_bytes": 52 * n, "achieved_gbs": gbs,
             "peak_gbs": peak, "frac": gbs / peak, "l2": "flushed before each timed call",
             "traffic": traffic_from_profiles("compaction_bcc128") if cells == 128 else None,
-            "traffic_what": "DRAM bytes read + written by one matter_kernel launch (ncu, profiles/compaction_bcc128.md)",
+            "traffic_what": "DRAM bytes read + written by one matter_kernel launch on this box (one ncu capture)",
             "timed": "whole call (loop upload, matter kernel, totals read back) with CUDA events",
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if pk else "fallback 6650 GB/s"}
 
